@@ -1,0 +1,338 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 lattice Boltzmann engine on LBFlow's headline workload.
+
+Workload (default): single-phase D3Q19 MRT in a synthetic porous cube of 256^3
+voxels -- seeded N(0,1) noise, periodic Gaussian filter sigma = 3, threshold at
+porosity 0.22, isolated fluid removed; fully periodic, tau = 1, g_x = 1e-5,
+FP64 plain path.  A step is one stream-collide update of every fluid node.
+
+Metric: fluid MLUPS (fluid nodes x steps / seconds / 1e6), the definition of
+the reference's scripts/performance.py:80-85.  `value` is device-timed (CUDA
+events on the engine's stream, inputs resident in HBM); `e2e` is the same
+metric through the C ABI from host buffers (geometry upload, initialization,
+every step's flux/mass read-back, final field download); `roofline` relates
+the step kernel's algorithmic bytes to the measured HBM bandwidth.
+
+    python bench.py [--steps K] [--warmup W] [--gpus N] [--storage fp64|fp32|fp16|bf16]
+    python bench.py --impl reference      # the reference solver on the host cores
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = 'D3Q19 MRT fluid MLUPS (256^3 porous cube, porosity 0.22)'
+# Algorithmic bytes per fluid-node update: read + write Q populations, plus
+# the 4-byte link information (2*Q*s + 4).
+ALG_BYTES = {'fp64': 2 * 19 * 8 + 4, 'fp32': 2 * 19 * 4 + 4, 'fp16': 2 * 19 * 2 + 4, 'bf16': 2 * 19 * 2 + 4}
+ELEM = {'fp64': 8, 'fp32': 4, 'fp16': 2, 'bf16': 2}
+REF_SAMPLE = dict(n=64, sigma=3.0, porosity=0.22, seed=0)
+
+
+def measured_peaks():
+    p = ROOT / 'MEASURED_PEAKS.json'
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d['hbm_gbs']), 'measured'
+    return 6650.0, 'fallback'
+
+
+def profile_traffic(storage):
+    """DRAM bytes per step-kernel launch from the committed ncu summary, if any."""
+    p = ROOT / 'profiles' / f'scsp_step_d3q19_mrt_{storage}_256.md'
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith('traffic_bytes_per_launch:'):
+            return float(line.split(':', 1)[1])
+    return None
+
+
+class ClockSampler:
+    """SM clocks and throttle reasons sampled (NVML, read-only) during the timed region."""
+    REASONS = {0x8: 'hw_slowdown', 0x40: 'hw_thermal_slowdown', 0x20: 'sw_thermal_slowdown',
+               0x4: 'sw_power_cap', 0x80: 'hw_power_brake_slowdown'}
+
+    def __init__(self, device, period=0.02):
+        self.device = device
+        self.period = period
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(self.device)
+            self._max = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        except Exception:
+            self._t = None
+        return self
+
+    def _run(self):
+        nv, h = self._nv, self._h
+        while not self._stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                self.samples.append((sm, r, pw))
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=2)
+
+    def summary(self):
+        if not self.samples:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': [], 'samples': 0}
+        reasons = set()
+        for _, r, _ in self.samples:
+            for bit, name in self.REASONS.items():
+                if r & bit:
+                    reasons.add(name)
+        return {'sm_mhz': statistics.median(s[0] for s in self.samples), 'sm_max_mhz': self._max,
+                'reasons': sorted(reasons), 'samples': len(self.samples),
+                'power_w_max': max(s[2] for s in self.samples)}
+
+
+def make_geometry(n, sigma, porosity, seed):
+    from lbflow_b200.geometry import porous_medium
+    fluid = porous_medium((n, n, n), sigma=sigma, porosity=porosity, seed=seed)
+    return np.where(fluid, 75, 255).astype(np.uint8)
+
+
+LABELS = {75: ('GV', 1e-5, 1, 0), 255: ('SD', 90.0, 0, 0)}
+
+
+def reference_run(workdir, geometry, steps, collision='MRT'):
+    """Run the reference LBFlow binary once; return (fluid_nodes, steps, numerical seconds)."""
+    exe = ROOT / 'oracle' / '_ref' / 'LBFlow'
+    nz, ny, nx = geometry.shape
+    workdir.mkdir(parents=True, exist_ok=True)
+    geometry.tofile(workdir / 'geometry.raw')
+    prm = f'''gridFile "geometry.raw";
+dimension {nz} {ny} {nx};
+directions 19;
+fileType "uint8";
+latticeLen 1;
+startTime 0;
+endTime {steps};
+writeInterval {steps};
+reportInterval {steps};
+restartInterval {steps * 10};
+stopError 1e-6;
+outPath "field";
+logPath ".";
+reportDir 0;
+reportSlice 1 {nx - 2};
+fluidModel "scsp";
+equilModel "{collision}";
+rexlationTime 1;
+latticeSpeed 1;
+alpha0 0.33333333333333331;
+density 1;
+contactAngle 90;
+surfaceTension 0;
+interfaceThickness 0.7;
+75 "GV" "1e-5" "1" "0"
+255 "SD" "90" "N/A" "N/A"
+'''
+    (workdir / 'input.prm').write_text(prm)
+    r = subprocess.run([str(exe), 'input.prm'], cwd=workdir, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError('reference run failed: ' + r.stdout[-500:])
+    t = [json.loads(l[len('LBFlowTiming '):]) for l in r.stdout.splitlines() if l.startswith('LBFlowTiming ')][0]
+    return t['fluid_nodes'], t['completed_steps'], t['numerical_seconds_max']
+
+
+def reference_sample(steps, procs):
+    """The reference solver on a bounded sample: `procs` concurrent single-rank runs
+    of the 64^3 crop of the same recipe; aggregate fluid MLUPS."""
+    exe = ROOT / 'oracle' / '_ref' / 'LBFlow'
+    if not exe.exists():
+        return None, 'reference binary oracle/_ref/LBFlow is not built'
+    g = make_geometry(REF_SAMPLE['n'], REF_SAMPLE['sigma'], REF_SAMPLE['porosity'], REF_SAMPLE['seed'])
+    with tempfile.TemporaryDirectory() as d:
+        import concurrent.futures as cf
+        with cf.ThreadPoolExecutor(procs) as ex:
+            res = list(ex.map(lambda k: reference_run(Path(d) / f'r{k}', g, steps), range(procs)))
+    nodes = sum(r[0] * r[1] for r in res)
+    secs = max(r[2] for r in res)
+    return dict(value=nodes / secs / 1e6, unit='MLUPS', cores=procs, kind='reference',
+                sample=f'{procs} x reference LBFlow (1 rank each) on the 64^3 crop of the same recipe '
+                       f'(sigma 3, porosity 0.22, seed 0, {res[0][0]} fluid nodes), MRT FP64, {steps} steps'), None
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get('RANK', '0'))
+    if rank != 0:
+        return 0
+    procs = max(1, min(os.cpu_count() or 1, 16))
+    steps = max(1, args.steps + args.warmup)
+    base, why = reference_sample(steps, procs)
+    cfg = dict(workload='D3Q19 MRT FP64 porous cube, reference solver on a 64^3 sample',
+               porosity=0.22, sigma=3, tau=1.0, g_x=1e-5)
+    if base is None:
+        print(json.dumps({'impl': 'reference', 'unavailable': why}))
+        return 0
+    line = dict(impl='reference', metric=METRIC, value=base['value'], unit='MLUPS', n_gpus=args.gpus,
+                steps=args.steps, warmup=args.warmup, ms_per_step=None, higher_is_better=True,
+                scaling='weak', vs_baseline=None, dtype='f64', data='synthetic', config=cfg,
+                cpu_baseline=base, e2e=dict(value=base['value'], unit='MLUPS', h2d_bytes_per_step=0,
+                                            d2h_bytes_per_step=0))
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=5000)
+    ap.add_argument('--warmup', type=int, default=5)
+    ap.add_argument('--impl', default='ours', choices=('ours', 'reference'))
+    ap.add_argument('--storage', default='fp64', choices=('fp64', 'fp32', 'fp16', 'bf16'))
+    ap.add_argument('--collision', default='MRT', choices=('MRT', 'SRT'))
+    ap.add_argument('--size', type=int, default=256)
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-e2e', action='store_true')
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == 'reference':
+        return run_reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group('nccl', timeout=timedelta(seconds=120), device_id=torch.device('cuda', local))
+
+    from lbflow_b200 import Engine
+    geometry = make_geometry(args.size, 3.0, 0.22, seed=rank)
+    N = geometry.size
+    eng = Engine(geometry, LABELS, model='scsp', collision=args.collision, tau=(1.0,), rho=(1.0,),
+                 storage=args.storage, device=local)
+    nf = eng.fluid_nodes
+    eng.initialize()
+    eng.step(args.warmup)
+    eng.synchronize()
+    eng.check()
+
+    stream = torch.cuda.ExternalStream(eng.stream, device=torch.device('cuda', local))
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        t0.record(stream)
+        for k in range(args.steps):
+            ev[k][0].record(stream)
+            eng.step(1)
+            ev[k][1].record(stream)
+        t1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    total_ms = t0.elapsed_time(t1)
+    launch_ms = statistics.fmean(a.elapsed_time(b) for a, b in ev)
+    eng.check()
+    if world > 1:
+        tt = torch.tensor([total_ms], device='cuda')
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+        nn = torch.tensor([float(nf)], device='cuda', dtype=torch.float64)
+        dist.all_reduce(nn)
+        nf_all = float(nn.item())
+    else:
+        nf_all = float(nf)
+    value = nf_all * args.steps / (total_ms / 1e3) / 1e6
+
+    peak, peak_kind = measured_peaks()
+    bytes_launch = nf * ALG_BYTES[args.storage]
+    achieved = bytes_launch / (launch_ms / 1e3) / 1e9
+    traffic = profile_traffic(args.storage)
+
+    e2e = None
+    if not args.no_e2e:
+        eng.close()
+        e2e = end_to_end(geometry, args, local)
+
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        base, _ = reference_sample(steps=100, procs=1)
+
+    if rank == 0:
+        clk = clocks.summary()
+        line = dict(metric=METRIC, value=value, unit='MLUPS', n_gpus=world, steps=args.steps,
+                    warmup=args.warmup, ms_per_step=total_ms / args.steps, higher_is_better=True,
+                    scaling='weak', vs_baseline=None, dtype=args.storage.replace('fp', 'f'),
+                    data='synthetic',
+                    config=dict(workload=f'D3Q19 {args.collision} single-phase porous cube {args.size}^3, '
+                                         f'{args.storage} populations',
+                                nx=args.size, ny=args.size, nz=args.size, porosity=0.22, sigma=3,
+                                tau=1.0, g_x=1e-5, fluid_nodes=nf, total_voxels=N,
+                                parallelism=f'replicas x{world}' if world > 1 else 'single GPU',
+                                l2='inputs larger than L2 (populations %.2f GB)' % (2 * nf * 19 * ELEM[args.storage] / 1e9)),
+                    roofline=dict(bound='hbm', achieved=achieved, peak=peak, unit='GB/s',
+                                  frac=achieved / peak, traffic=traffic, peak_kind=peak_kind,
+                                  bytes_per_launch=bytes_launch, launch_ms=launch_ms),
+                    gpu_launches=args.steps,
+                    clocks=clk, e2e=e2e, cpu_baseline=base)
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def end_to_end(geometry, args, device):
+    """Same metric through the C ABI with host buffers: geometry upload and
+    classification, initialization, K steps each followed by the read-back of
+    the step's flux and mass sums, then the final density/velocity download."""
+    from lbflow_b200 import Engine
+    import torch
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    eng = Engine(geometry, LABELS, model='scsp', collision=args.collision, tau=(1.0,), rho=(1.0,),
+                 storage=args.storage, device=device)
+    eng.initialize()
+    for _ in range(args.steps):
+        eng.step(1, macros=True)
+        eng.flux_sums()
+    r0, _, u = eng.macros()
+    eng.check()
+    dt = time.perf_counter() - t
+    nf = eng.fluid_nodes
+    eng.close()
+    h2d = geometry.nbytes + 256 * 24
+    d2h = 9 * 8 * args.steps + r0.nbytes + u.nbytes
+    return dict(value=nf * args.steps / dt / 1e6, unit='MLUPS',
+                h2d_bytes_per_step=h2d / args.steps, d2h_bytes_per_step=d2h / args.steps,
+                seconds=dt)
+
+
+if __name__ == '__main__':
+    sys.exit(main())

@@ -1,0 +1,175 @@
+/* lbflow.h -- C ABI of the B200 lattice Boltzmann engine.
+ *
+ * The engine is the solver core of LBFlow (zhou1800/lbflow) rebuilt for one
+ * NVIDIA B200: it replaces the per-step work of SCSP::Run and ColorFluid::Run
+ * (solver/src/lbm/scsp.cpp:46-114, solver/src/lbm/colorfluid.cpp:109-212)
+ * -- streaming, bounce-back, macroscopic variables, body force, collision, the
+ * color-gradient operators and the reductions behind reports and convergence.
+ * The C++11 host driver (the LBFlow command line) keeps the parameter file,
+ * geometry, VTI and checkpoint formats and calls only the functions below.
+ *
+ * Conventions
+ *  - Plain C types only; host arrays are copied in or out and never retained.
+ *  - Dense host arrays use the reference's layout: voxel v = (z*ny + y)*nx + x,
+ *    populations [phase][q][v] with the reference's q ordering
+ *    (solver/src/grid/gridspace.cpp:82-144), vectors as [3][v] in x, y, z order.
+ *  - Every function returns LBF_OK (0) or a negative LBF_E* code; the message
+ *    is available from lbf_last_error().  Nothing traps on the device: numeric
+ *    failures raise bits of a device error word, read by lbf_status().
+ *  - One engine = one geometry on one GPU, driven by one host thread; all work
+ *    is queued on the engine's CUDA stream.
+ */
+#ifndef LBFLOW_H
+#define LBFLOW_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBF_ABI_VERSION 1
+
+/* Return codes. */
+enum {
+    LBF_OK = 0,
+    LBF_EINVAL = -1,    /* invalid argument or unsupported option */
+    LBF_ECUDA = -2,     /* CUDA runtime failure (message from the runtime) */
+    LBF_ESTATE = -3,    /* call out of order (e.g. step before initialize) */
+    LBF_ENUMERIC = -4,  /* device error word is non-zero (see lbf_status) */
+    LBF_ENOMEM = -5     /* device allocation failed */
+};
+
+/* Geometry label types: the bit values of FilePrm::IDXTYPE
+ * (solver/inc/file/fileprm.h:44-53). */
+enum {
+    LBF_VD = 0x1, LBF_GV = 0x2, LBF_PB = 0x4, LBF_VB = 0x8,
+    LBF_AB = 0x10, LBF_BB = 0x20, LBF_HF = 0x40, LBF_SD = 0x80
+};
+
+enum { LBF_MODEL_SCSP = 0, LBF_MODEL_COLOR = 1 };
+enum { LBF_SRT = 0, LBF_MRT = 1 };
+/* Population storage.  FP64 is the plain path (FP64 arithmetic).  The others
+ * store shifted deviations f_q - w_q*rho0, scaled per direction, and collide
+ * in FP32; reductions stay FP64. */
+enum { LBF_STORE_FP64 = 0, LBF_STORE_FP16 = 1, LBF_STORE_BF16 = 2, LBF_STORE_FP32 = 3 };
+
+/* Device error word bits (the reference's throw conditions). */
+enum {
+    LBF_ERR_DENSITY = 1u << 0,    /* non-finite or non-positive density */
+    LBF_ERR_COMPONENT = 1u << 1,  /* negative component density (color) */
+    LBF_ERR_TAU = 1u << 2,        /* local relaxation time <= 0.5 (color) */
+    LBF_ERR_VELOCITY = 1u << 3    /* non-finite velocity (color) */
+};
+
+/* lbf_step flags: what the LAST step of the call also writes. */
+enum {
+    LBF_STEP_MACROS = 1u << 0,    /* density(ies) and velocity of that step */
+    LBF_STEP_ADJACENT = 1u << 1   /* velocity (and phase indicator) kept as the
+                                     "adjacent" history of the next report */
+};
+
+/* One geometry label: a line `N "TYPE" "value" "dir" "phase"` of input.prm
+ * after FilePrm::IDXVAL parsing (solver/src/file/fileprm.cpp:633-670). */
+typedef struct {
+    int32_t type;     /* LBF_VD ... LBF_SD; 0 = label not defined */
+    int32_t dir;      /* GV: lattice direction of the force */
+    int32_t phase;    /* VD/GV: fluid phase */
+    int32_t reserved;
+    double value;     /* GV: force magnitude; SD: contact angle in degrees */
+} lbf_label;
+
+typedef struct {
+    uint32_t dims;        /* 2 (D2Q9) or 3 (D3Q19) */
+    uint32_t nx, ny, nz;  /* nz = 1 in 2D; nx, ny <= 2048, nz <= 1024 */
+    uint32_t model;       /* LBF_MODEL_SCSP or LBF_MODEL_COLOR */
+    uint32_t collision;   /* LBF_SRT or LBF_MRT */
+    uint32_t storage;     /* LBF_STORE_* */
+    int32_t device;       /* CUDA device ordinal */
+    double tau[2];        /* relaxation times (tau[1]: color phase 1) */
+    double rho[2];        /* reference densities */
+    double alpha0;        /* color: rest weight of phase 0 */
+    double sigma;         /* color: surface tension */
+    double beta;          /* color: recoloring parameter */
+} lbf_config;
+
+typedef struct lbf_engine lbf_engine;
+
+/* Build an engine: classify links (Simulator::buildIb, simulator.cpp:386-436,
+ * and Grid::calcAdjI periodic wrap, solver/inc/grid/grid.h:179-189), pack the
+ * fluid nodes and allocate device state.  geometry holds nx*ny*nz labels.
+ * Replaces the Simulator/SCSP/ColorFluid constructors
+ * (simulator.cpp:17-38, scsp.cpp:22-44, colorfluid.cpp:20-107). */
+int lbf_create(const lbf_config *cfg, const lbf_label labels[256],
+               const uint8_t *geometry, lbf_engine **out);
+void lbf_destroy(lbf_engine *e);
+
+/* The t = 0 stage of Run: initialize, calcMacroVar, bodyForce and the initial
+ * collision (scsp.cpp:60-71, 116-134; colorfluid.cpp:123-138, 214-236).  The
+ * t = 0 macroscopic fields are kept for lbf_get_macros. */
+int lbf_initialize(lbf_engine *e);
+
+/* nsteps steps of the Run loop body: streaming, bounce-back, calcMacroVar,
+ * bodyForce, collision (scsp.cpp:75-104; colorfluid.cpp:142-198).  flags
+ * (LBF_STEP_*) apply to the last step of the call. */
+int lbf_step(lbf_engine *e, uint32_t nsteps, uint32_t flags);
+
+/* Post-collision populations, dense FP64 [phase][q][voxel], the checkpoint
+ * content of saveRst/loadRst (scsp.cpp:277-302; colorfluid.cpp:766-812).
+ * Solid voxels are written as 0 and ignored on load.  n = element count. */
+int lbf_get_populations(lbf_engine *e, double *host, size_t n);
+int lbf_set_populations(lbf_engine *e, const double *host, size_t n);
+
+/* Macroscopic fields of the last step that wrote them (LBF_STEP_MACROS or
+ * lbf_initialize), dense: rho0 (density, or rho_0 for color), rho1 (color
+ * only; may be NULL), u [3][voxel]; zero on solid voxels as in the VTI output
+ * (filevti.cpp:113-172).  Any pointer may be NULL. */
+int lbf_get_macros(lbf_engine *e, double *rho0, double *rho1, double *u);
+
+/* Device reductions of Simulator::updateConvergence (simulator.cpp:248-325).
+ * first != 0 only records the current velocity (and phase indicator) as the
+ * previous report.  Otherwise out = { sum (u-u_prev)^2, sum u^2,
+ * sum (u-u_adj)^2, max |ind-ind_prev|, max |ind-ind_adj|, 0 } over all voxels
+ * and components, then the current fields become the previous report. */
+int lbf_convergence(lbf_engine *e, int first, double out[6]);
+
+/* Slice sums of SCSP::report / ColorFluid::report (scsp.cpp:325-341;
+ * colorfluid.cpp:841-867) along axis (0 = x, 1 = y, 2 = z) between slices lo
+ * and hi: out = { sum u_axis over lo..hi, sum rho0 over lo..hi,
+ * sum rho1 over lo..hi, sum rho0 at lo, sum rho1 at lo, sum rho0 at hi,
+ * sum rho1 at hi, fluid count at lo, fluid count at hi, fluid count lo..hi }.
+ * Single phase: rho1 terms are 0. */
+int lbf_report_sums(lbf_engine *e, uint32_t axis, uint32_t lo, uint32_t hi, double out[10]);
+
+/* Pore measures of scripts/porous_media.py:20-44 on the last macros, summed
+ * over fluid voxels: out = { sum u_x, sum u_y, sum u_z, sum phi0 u_x,
+ * sum phi0 u_y, sum phi0 u_z, sum rho0, sum rho1, sum phi0 } with
+ * phi0 = rho0/(rho0+rho1) (1 for single phase).  Divide by nx*ny*nz for the
+ * Darcy velocity; permeability K = nu <u_x> / g_x. */
+int lbf_flux_sums(lbf_engine *e, double out[9]);
+
+/* Link classification as the kernels use it: per voxel, bit (q-1) set when
+ * the voxel is fluid and its neighbour x + e_q is a BB/SD solid
+ * (simulator.cpp:405-415).  n = nx*ny*nz. */
+int lbf_link_mask(lbf_engine *e, uint32_t *host, size_t n);
+
+/* Waits for queued work and returns the device error word (LBF_ERR_* bits). */
+int lbf_status(lbf_engine *e, uint32_t *bits);
+
+/* Number of fluid nodes (the reference's fluid_nodes, simulator.cpp:47-56). */
+uint64_t lbf_fluid_nodes(const lbf_engine *e);
+/* Device bytes held by the engine. */
+uint64_t lbf_device_bytes(const lbf_engine *e);
+/* Message of the last failed call on e (or of lbf_create when e is NULL). */
+const char *lbf_last_error(const lbf_engine *e);
+/* Wait for all queued work of the engine. */
+int lbf_synchronize(lbf_engine *e);
+/* The CUDA stream (a cudaStream_t) all of the engine's work is queued on,
+ * for callers that time or order work against it. */
+void *lbf_stream(const lbf_engine *e);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LBFLOW_H */

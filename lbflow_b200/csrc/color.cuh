@@ -1,0 +1,336 @@
+// Two-phase color-gradient kernels (ColorFluid, solver/src/lbm/colorfluid.cpp).
+//
+// A step needs the phase field phi = (rho0 - rho1)/rho of every neighbour
+// after streaming, so it runs as two launches over the fluid nodes:
+//   pass 1  color_phase:   pull both components (with bounce-back), write phi;
+//   pass 2  color_collide: pull again, macros, collision of the total
+//           distribution, color gradient (legacy interior stencil or the
+//           geometric wall rotation), perturbation and recoloring.
+// Solid voxels read as phi = 86 (SOLID_DENS_N, colorfluid.cpp:49).
+#pragma once
+#include "kernels.cuh"
+
+namespace lbf {
+
+struct ColorParams {
+    double ai[2][19];      // phase weights (ColorFluid::initPhi, colorfluid.cpp:1131-1150)
+    double rho_ref[2];     // reference densities
+    double relax0, relax1; // tau_k / 2 (colorfluid.cpp:241-242)
+    int uniform_tau;       // tau0 == tau1: fixed MRT rates (colorfluid.cpp:317-322)
+    MrtCoef mrt;           // coefficients of the uniform rates
+    double ak;             // 2.25 sigma (colorfluid.cpp:305)
+    double beta;           // recoloring parameter
+};
+
+struct ColorWall {
+    const uint16_t* __restrict__ angle_id;  // per fluid node; 0 = not next to a solid
+    const double* __restrict__ angles;      // [id][2] = cos, sin of the mean contact angle
+    const double* __restrict__ tib;         // per wall-normal code: TibNorm, row-major, reference {z,y,x} order
+};
+
+constexpr double kSolidPhi = 86.0;
+
+// Non-contracted IEEE arithmetic (never fused into FMA).
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float xmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float xadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float xsub(float a, float b) { return __fsub_rn(a, b); }
+
+// Normal code of a wall node: n = -sum e_q over solid links, components in
+// the reference order (n0, n1, n2) = {z,y,x} in 3D and (n0, n1) = {y,x} in 2D,
+// each in [-5, 5] (3D) or [-3, 3] (2D).
+template <class L> __host__ __device__ inline int normal_code(int n0, int n1, int n2)
+{
+    return L::D == 3 ? ((n0 + 5) * 11 + (n1 + 5)) * 11 + (n2 + 5) : (n0 + 3) * 7 + (n1 + 3);
+}
+template <class L> constexpr int normal_codes() { return L::D == 3 ? 11 * 11 * 11 : 7 * 7; }
+
+// Pass 1: phase field.  PULL = false reads the node's own values (t = 0).
+template <class L, class S, bool PULL>
+__global__ void __launch_bounds__(128)
+color_phase(const Grid g, const typename S::T* __restrict__ fin, double* __restrict__ phi,
+            uint32_t* __restrict__ err)
+{
+    using R = typename S::R;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.nf) return;
+    int x, y, z;
+    unpack(__ldg(&g.coord[i]), x, y, z);
+    R f0[L::Q], f1[L::Q];
+    uint32_t nbr[L::Q];
+    gather<L, S, PULL>(g, fin, i, x, y, z, f0, nbr, R(0));
+    gather<L, S, PULL>(g, fin + (size_t)L::Q * g.nfp, i, x, y, z, f1, nbr, R(0));
+    R d0 = f0[0], d1 = f1[0];
+#pragma unroll
+    for (int q = 1; q < L::Q; ++q) { d0 += f0[q]; d1 += f1[q]; }
+    const R dt = d0 + d1;
+    if (!isfinite(d0) || !isfinite(d1) || !isfinite(dt) || !(dt > R(0))) atomicOr(err, kErrDensity);
+    if (d0 < R(-1e-10) * dt || d1 < R(-1e-10) * dt) atomicOr(err, kErrComponent);
+    phi[i] = (double)((d0 - d1) / dt);
+}
+
+// Pass 2: collision, gradient, perturbation and recoloring.
+// COLL: 0 = SRT, 1 = MRT.  PULL = false is the t = 0 collision.
+template <class L, class S, int COLL, bool PULL>
+__global__ void __launch_bounds__(128)
+color_collide(const Grid g, const Force F, const ColorParams P, const ColorWall W,
+              const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
+              const double* __restrict__ phi, Macros mo, const int out, uint32_t* __restrict__ err)
+{
+    using R = typename S::R;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.nf) return;
+    int x, y, z;
+    unpack(__ldg(&g.coord[i]), x, y, z);
+    R f0[L::Q], f1[L::Q];
+    uint32_t nbr[L::Q];
+    gather<L, S, PULL>(g, fin, i, x, y, z, f0, nbr, R(0));
+    gather<L, S, PULL>(g, fin + (size_t)L::Q * g.nfp, i, x, y, z, f1, nbr, R(0));
+    if (!PULL) {
+        // t = 0: neighbours by direct lookup (the pull above read local values).
+#pragma unroll
+        for (int q = 1; q < L::Q; ++q) {
+            bool fluid;
+            const uint32_t j = lookup(g, wrap(x + L::ex(q), g.nx), wrap(y + L::ey(q), g.ny),
+                                      L::D == 3 ? wrap(z + L::ez(q), g.nz) : 0, fluid);
+            nbr[q] = fluid ? j : 0xffffffffu;
+        }
+    }
+
+    // ColorFluid::calcMacroVar (colorfluid.cpp:238-290) and bodyForce (:736-750).
+    R d0 = f0[0], d1 = f1[0];
+#pragma unroll
+    for (int q = 1; q < L::Q; ++q) { d0 += f0[q]; d1 += f1[q]; }
+    const R dt = d0 + d1;
+    const R phi_i = (d0 - d1) / dt;
+    const R tau = (R(1) + phi_i) * R(P.relax0) + (R(1) - phi_i) * R(P.relax1);
+    if (!isfinite(tau) || !(tau > R(0.5))) atomicOr(err, kErrTau);
+    R Fv[3];
+    if (F.uniform) { Fv[0] = R(F.fx); Fv[1] = R(F.fy); Fv[2] = R(F.fz); }
+    else {
+        const double* lf = F.label_force + 3 * __ldg(&F.label[i]);
+        Fv[0] = R(lf[0]); Fv[1] = R(lf[1]); Fv[2] = R(lf[2]);
+    }
+    // Velocity components accumulated in the reference's component order.
+    R u[3] = {R(0), R(0), R(0)};
+#pragma unroll
+    for (int a = 0; a < L::D; ++a) {
+        R v = R(0);
+#pragma unroll
+        for (int q = 1; q < L::Q; ++q) {
+            const int e = comp<L>(q, a);
+            if (e == 1) v += f0[q] + f1[q];
+            else if (e == -1) v -= f0[q] + f1[q];
+        }
+        u[a] = v / dt;
+    }
+    if (!isfinite(u[0]) || !isfinite(u[1]) || !isfinite(u[2])) atomicOr(err, kErrVelocity);
+#pragma unroll
+    for (int a = 0; a < L::D; ++a) u[a] += Fv[a] * R(0.5) / dt;
+
+    if (out & kOutMacros) {
+        mo.rho0[i] = (double)d0;
+        mo.rho1[i] = (double)d1;
+        mo.ind[i] = (double)phi_i;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) mo.u[(size_t)a * g.nfp + i] = (double)u[a];
+    }
+    if (out & kOutAdjacent) {
+        mo.indadj[i] = (double)phi_i;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) mo.uadj[(size_t)a * g.nfp + i] = (double)u[a];
+    }
+
+    // ColorFluid::collision (colorfluid.cpp:334-387): collide the total.
+    const R usq = u[2] * u[2] + u[1] * u[1] + u[0] * u[0];
+    const R uf = u[2] * Fv[2] + u[1] * Fv[1] + u[0] * Fv[0];
+    R fT[L::Q], fu0[L::Q], src[L::Q];
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) {
+        fT[q] = f0[q] + f1[q];
+        const R eu = R(L::ex(q)) * u[0] + R(L::ey(q)) * u[1] + R(L::ez(q)) * u[2];
+        const R ef = R(L::ex(q)) * Fv[0] + R(L::ey(q)) * Fv[1] + R(L::ez(q)) * Fv[2];
+        fu0[q] = d0 * R(P.ai[0][q]) + d1 * R(P.ai[1][q]);
+        const R feq = fu0[q] + dt * R(w<L>(q)) * (R(3) * eu + R(4.5) * eu * eu - R(1.5) * usq);
+        src[q] = R(w<L>(q)) * (R(3) * (ef - uf) + R(9) * eu * ef);
+        fT[q] = COLL == 0 ? fT[q] : feq - fT[q];   // MRT: residual
+        if (COLL == 0) {
+            fT[q] += (feq - fT[q]) / tau;
+            fT[q] += (R(1) - R(0.5) / tau) * src[q];
+        }
+    }
+    if (COLL == 1) {
+        R mr[L::Q], ms[L::Q], c[L::Q];
+        mforward<R>(fT, mr);
+        mforward<R>(src, ms);
+        // fT currently holds the residual; rebuild the total before the update.
+#pragma unroll
+        for (int q = 0; q < L::Q; ++q) fT[q] = f0[q] + f1[q];
+        if (P.uniform_tau) {
+#pragma unroll
+            for (int k = 0; k < L::Q; ++k) c[k] = R(P.mrt.cr[k]) * mr[k] + R(P.mrt.cs[k]) * ms[k];
+        } else {
+            // Simulator::getMRTS at the local tau (simulator.cpp:199-216).
+            const R su = R(1) / tau;
+            const R sq = R(8) * (R(2) - su) / (R(8) - su);
+#pragma unroll
+            for (int k = 0; k < L::Q; ++k) {
+                const R s = L::rowclass(k) == kConserved ? R(0) : (L::rowclass(k) == kShear ? su : sq);
+                c[k] = (s * mr[k] + (R(1) - R(0.5) * s) * ms[k]) * R(P.mrt.inv_n[k]);
+            }
+        }
+        minverse_add<R>(c, fT);
+    }
+
+    // ColorFluid::colorGradient (colorfluid.cpp:435-570), gradient in the
+    // reference component order gr[0..D-1] = {z,y,x} / {y,x}.  The gradient
+    // and the wall rotation use non-contracted IEEE operations in the
+    // reference's order: the rotation angle is undefined when the in-plane
+    // gradient vanishes, so exact cancellations must stay exact.
+    R gr[3] = {R(0), R(0), R(0)};
+    const uint16_t wid = __ldg(&W.angle_id[i]);
+    R phin[L::Q];
+#pragma unroll
+    for (int q = 1; q < L::Q; ++q) phin[q] = nbr[q] == 0xffffffffu ? R(kSolidPhi) : R(__ldg(&phi[nbr[q]]));
+#pragma unroll
+    for (int d = 0; d < L::D; ++d) {
+#pragma unroll
+        for (int k = 0; k < L::NRELD; ++k) {
+            const int q = L::reld(d, k);
+            const int e = comp<L>(q, L::D - 1 - d);
+            R term = phin[q];
+            if (wid) {
+                if (phin[q] == R(kSolidPhi)) continue;
+                term = xsub(phin[q], phi_i);
+            }
+            if (e == 1) gr[d] = xadd(gr[d], xmul(R(w<L>(q)), term));
+            else gr[d] = xsub(gr[d], xmul(R(w<L>(q)), term));
+        }
+    }
+    R n2 = R(0);
+#pragma unroll
+    for (int d = 0; d < L::D; ++d) gr[d] = xmul(gr[d], R(3));
+#pragma unroll
+    for (int d = 0; d < L::D; ++d) n2 = xadd(n2, xmul(gr[d], gr[d]));
+    const R norm = sqrt(n2);
+    if (wid) {
+        const double* cs = W.angles + 2 * wid;
+        const R cA = R(cs[0]), sA = R(cs[1]);
+        int nn[3] = {0, 0, 0};   // normal in reference order
+#pragma unroll
+        for (int q = 1; q < L::Q; ++q)
+            if (nbr[q] == 0xffffffffu) {
+#pragma unroll
+                for (int d = 0; d < L::D; ++d) nn[d] -= comp<L>(q, L::D - 1 - d);
+            }
+        const int code = normal_code<L>(nn[0], nn[1], nn[2]);
+        if (L::D == 3) {
+            const double* T = W.tib + 9 * code;
+            R gn[3];
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                R s = R(0);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) s = xadd(s, xmul(R(T[3 * r + k]), gr[k]));
+                gn[r] = s;
+            }
+            // RotateTx3D(-gn0, gn1) (fn.cpp:129-139).
+            R c = R(1), sn = R(0);
+            const R o = -gn[0];
+            const R h = sqrt(xadd(xmul(o, o), xmul(gn[1], gn[1])));
+            if (h != R(0)) { c = gn[1] / h; sn = o / h; }
+            const R tx[9] = {c, -sn, R(0), sn, c, R(0), R(0), R(0), R(1)};
+            // tInv = TibNormInv * txInv with TibNormInv = TibNorm^T.
+            R ti[9];
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int col = 0; col < 3; ++col) {
+                    R s = R(0);
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) s = xadd(s, xmul(R(T[3 * k + r]), tx[3 * k + col]));
+                    ti[3 * r + col] = s;
+                }
+            const R t[3] = {R(0), xmul(norm, sA), xmul(norm, cA)};
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                R s = R(0);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) s = xadd(s, xmul(ti[3 * r + k], t[k]));
+                gr[r] = s;
+            }
+        } else {
+            const double* T = W.tib + 4 * code;
+            const R gn0 = xadd(xadd(R(0), xmul(R(T[0]), gr[0])), xmul(R(T[1]), gr[1]));
+            R t[2];
+            if (gn0 >= R(0)) { t[0] = xmul(norm, sA); t[1] = xmul(norm, cA); }
+            else { t[0] = xmul(-norm, sA); t[1] = xmul(norm, cA); }
+            // TibNormInv = TibNorm^T.
+            const R g0 = xadd(xadd(R(0), xmul(R(T[0]), t[0])), xmul(R(T[2]), t[1]));
+            const R g1 = xadd(xadd(R(0), xmul(R(T[1]), t[0])), xmul(R(T[3]), t[1]));
+            gr[0] = g0; gr[1] = g1;
+        }
+    }
+
+    // Perturbation and cosine recoloring (colorfluid.cpp:399-428).
+    const R dens0T = d0 / dt;
+    typename S::T* o0 = fout;
+    typename S::T* o1 = fout + (size_t)L::Q * g.nfp;
+    if (norm > R(1e-9)) {
+        const R betaDens01TT = R(P.beta) * dens0T * d1 / dt;
+        const R AkNorm = R(P.ak) * norm / tau;
+#pragma unroll
+        for (int q = 0; q < L::Q; ++q) {
+            R angle = R(0);
+#pragma unroll
+            for (int d = 0; d < L::D; ++d) {
+                const int e = comp<L>(q, L::D - 1 - d);
+                if (e == 1) angle += gr[d];
+                else if (e == -1) angle -= gr[d];
+            }
+            angle /= norm;
+            fT[q] += AkNorm * (R(w<L>(q)) * angle * angle - R(L::B(q)));
+            if (q != 0 && !axis_dir<L>(q)) angle /= R(1.4142135623730951);
+            const R a0 = dens0T * fT[q] + betaDens01TT * angle * fu0[q];
+            S::store(o0 + (size_t)q * g.nfp + i, a0, q, R(0));
+            S::store(o1 + (size_t)q * g.nfp + i, fT[q] - a0, q, R(0));
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < L::Q; ++q) {
+            const R a0 = dens0T * fT[q];
+            S::store(o0 + (size_t)q * g.nfp + i, a0, q, R(0));
+            S::store(o1 + (size_t)q * g.nfp + i, fT[q] - a0, q, R(0));
+        }
+    }
+}
+
+// t = 0 populations of ColorFluid::initialize (colorfluid.cpp:214-236):
+// the node's phase gets ai_k,q rho_k - 1.5 w_q (e.F), the other phase 0.
+template <class L, class S>
+__global__ void color_init(const Grid g, const Force F, const ColorParams P,
+                           const uint8_t* __restrict__ phase, typename S::T* __restrict__ f)
+{
+    using R = typename S::R;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.nf) return;
+    double Fv[3];
+    if (F.uniform) { Fv[0] = F.fx; Fv[1] = F.fy; Fv[2] = F.fz; }
+    else { const double* lf = F.label_force + 3 * F.label[i]; Fv[0] = lf[0]; Fv[1] = lf[1]; Fv[2] = lf[2]; }
+    const int ph = phase[i];
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) {
+        double ef = 0.0;
+        if (L::D == 3) ef = L::ez(q) * Fv[2];
+        ef += L::ey(q) * Fv[1];
+        ef += L::ex(q) * Fv[0];
+        double v = P.ai[ph][q] * P.rho_ref[ph];
+        v -= 1.5 * (L::w36f(q) / 36.0) * ef;
+        S::store(f + ((size_t)ph * L::Q + q) * g.nfp + i, R(v), q, R(0));
+        S::store(f + ((size_t)(1 - ph) * L::Q + q) * g.nfp + i, R(0), q, R(0));
+    }
+}
+
+}  // namespace lbf

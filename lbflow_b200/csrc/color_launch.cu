@@ -1,0 +1,61 @@
+// Template instantiation and dispatch of the two-phase kernels.
+#include "internal.h"
+#include "../../include/lbflow.h"
+
+namespace lbf {
+
+namespace {
+template <class L, class S, int COLL>
+void dispatch(bool pull, int out, const ColorLaunch& a)
+{
+    using T = typename S::T;
+    const T* fin = static_cast<const T*>(a.fin);
+    T* fout = static_cast<T*>(a.fout);
+    const unsigned threads = 128, blocks = blocks_for(a.g.nf, threads);
+    if (blocks == 0) return;
+    if (pull) color_phase<L, S, true><<<blocks, threads, 0, a.stream>>>(a.g, fin, a.phi, a.err);
+    else color_phase<L, S, false><<<blocks, threads, 0, a.stream>>>(a.g, fin, a.phi, a.err);
+    if (pull)
+        color_collide<L, S, COLL, true><<<blocks, threads, 0, a.stream>>>(
+            a.g, a.F, a.P, a.W, fin, fout, a.phi, a.mo, out, a.err);
+    else
+        color_collide<L, S, COLL, false><<<blocks, threads, 0, a.stream>>>(
+            a.g, a.F, a.P, a.W, fin, fout, a.phi, a.mo, out, a.err);
+
+}
+
+template <class L, class S>
+void dispatch_coll(int collision, bool pull, int out, const ColorLaunch& a)
+{
+    if (collision == LBF_MRT) dispatch<L, S, 1>(pull, out, a);
+    else dispatch<L, S, 0>(pull, out, a);
+}
+}  // namespace
+
+void launch_color(int dims, int storage, int collision, bool pull, int out, const ColorLaunch& a)
+{
+    // The two-phase path stores full populations (FP64, or FP32 at reduced precision).
+    if (dims == 3) {
+        if (storage == LBF_STORE_FP64) dispatch_coll<D3Q19, StoreF64>(collision, pull, out, a);
+        else dispatch_coll<D3Q19, StoreF32Full>(collision, pull, out, a);
+    } else {
+        if (storage == LBF_STORE_FP64) dispatch_coll<D2Q9, StoreF64>(collision, pull, out, a);
+        else dispatch_coll<D2Q9, StoreF32Full>(collision, pull, out, a);
+    }
+}
+
+void launch_color_init(int dims, int storage, const Grid& g, const Force& F, const ColorParams& P,
+                       const uint8_t* phase, void* f, cudaStream_t s)
+{
+    const unsigned threads = 256, blocks = blocks_for(g.nf, threads);
+    if (blocks == 0) return;
+    if (dims == 3) {
+        if (storage == LBF_STORE_FP64) color_init<D3Q19, StoreF64><<<blocks, threads, 0, s>>>(g, F, P, phase, (double*)f);
+        else color_init<D3Q19, StoreF32Full><<<blocks, threads, 0, s>>>(g, F, P, phase, (float*)f);
+    } else {
+        if (storage == LBF_STORE_FP64) color_init<D2Q9, StoreF64><<<blocks, threads, 0, s>>>(g, F, P, phase, (double*)f);
+        else color_init<D2Q9, StoreF32Full><<<blocks, threads, 0, s>>>(g, F, P, phase, (float*)f);
+    }
+}
+
+}  // namespace lbf

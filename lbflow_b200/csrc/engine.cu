@@ -1,0 +1,778 @@
+// Host side of the C ABI (include/lbflow.h): geometry packing, link
+// classification, device state and the step / reduction drivers.
+#include "../../include/lbflow.h"
+#include "internal.h"
+#include "reduce.cuh"
+
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <utility>
+#include <vector>
+
+using namespace lbf;
+
+struct lbf_engine {
+    lbf_config cfg;
+    lbf_label labels[256];
+    int D = 3, Q = 19, phases = 1;
+    int nx = 0, ny = 0, nz = 0, W = 0;
+    size_t N = 0;
+    uint32_t nf = 0, nfp = 0;
+    std::vector<uint32_t> vox;      // voxel index of each fluid node
+    size_t elem = 8;                // bytes per stored population
+    void* f[2] = {nullptr, nullptr};
+    int cur = 0;
+    uint2* occ = nullptr;
+    uint32_t* coord = nullptr;
+    uint8_t* node_label = nullptr;
+    uint8_t* node_phase = nullptr;
+    double* label_force = nullptr;
+    double *rho0 = nullptr, *rho1 = nullptr, *u = nullptr, *uprev = nullptr, *uadj = nullptr;
+    double *ind = nullptr, *indprev = nullptr, *indadj = nullptr, *phi = nullptr;
+    uint16_t* angle_id = nullptr;
+    double* angles = nullptr;
+    double* tib = nullptr;
+    uint32_t* err = nullptr;
+    double* partial = nullptr;
+    double* red = nullptr;
+    double* h_red = nullptr;        // pinned
+    cudaStream_t stream = nullptr;
+    Force force{};
+    ScspParams sp{};
+    ColorParams cp{};
+    bool initialized = false;
+    uint64_t bytes = 0;
+    std::string last_error;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+int fail(lbf_engine* e, int code, const std::string& msg)
+{
+    if (e) e->last_error = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+#define LBF_CK(e, call)                                                                  \
+    do {                                                                                 \
+        cudaError_t err_ = (call);                                                       \
+        if (err_ != cudaSuccess)                                                         \
+            return fail(e, LBF_ECUDA, std::string(#call) + ": " + cudaGetErrorString(err_)); \
+    } while (0)
+
+template <class T>
+int dalloc(lbf_engine* e, T** p, size_t count)
+{
+    *p = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t r = cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T));
+    if (r != cudaSuccess)
+        return fail(e, r == cudaErrorMemoryAllocation ? LBF_ENOMEM : LBF_ECUDA,
+                    std::string("cudaMalloc: ") + cudaGetErrorString(r));
+    e->bytes += count * sizeof(T);
+    return LBF_OK;
+}
+
+// Reference lattice tables in reference component order ({y,x} / {z,y,x}),
+// used for host-side classification exactly as Simulator::buildIb does.
+const int kE9[9][3] = {{0,0,0},{0,1,0},{1,0,0},{0,-1,0},{-1,0,0},{1,1,0},{1,-1,0},{-1,-1,0},{-1,1,0}};
+const int kE19[19][3] = {{0,0,0},{0,0,1},{0,0,-1},{0,1,0},{0,-1,0},{1,0,0},{-1,0,0},
+    {0,1,1},{0,1,-1},{0,-1,1},{0,-1,-1},{1,0,1},{1,0,-1},{-1,0,1},{-1,0,-1},
+    {1,1,0},{1,-1,0},{-1,1,0},{-1,-1,0}};
+
+bool is_fluid(int t) { return t == LBF_VD || t == LBF_GV; }
+bool is_solid(int t) { return t == LBF_BB || t == LBF_SD; }
+
+// e_q component a (0 = x, 1 = y, 2 = z) of the reference tables.
+int ecomp(int D, int q, int a)
+{
+    if (D == 2) return a == 0 ? kE9[q][1] : (a == 1 ? kE9[q][0] : 0);
+    return kE19[q][2 - a];
+}
+
+// Simulator::getMRTS (simulator.cpp:199-216), legacy spectrum.
+void mrt_rates(int Q, double rt, double* s)
+{
+    const double su = 1.0 / rt;
+    const double sq = 8.0 * (2.0 - su) / (8.0 - su);
+    static const int cls9[9] = {0, 1, 1, 0, 2, 0, 2, 1, 1};
+    static const int cls19[19] = {0, 1, 1, 0, 2, 0, 2, 0, 2, 1, 1, 1, 1, 1, 1, 1, 2, 2, 2};
+    for (int k = 0; k < Q; ++k) {
+        const int c = Q == 9 ? cls9[k] : cls19[k];
+        s[k] = c == 0 ? 0.0 : (c == 1 ? su : sq);
+    }
+}
+
+template <class L>
+MrtCoef mrt_coef(double tau)
+{
+    MrtCoef m{};
+    double s[19];
+    mrt_rates(L::Q, tau, s);
+    for (int k = 0; k < L::Q; ++k) {
+        const double n = (double)rownorm2<L>(k);
+        m.cr[k] = s[k] / n;
+        m.cs[k] = (1.0 - 0.5 * s[k]) / n;
+        m.inv_n[k] = 1.0 / n;
+    }
+    return m;
+}
+
+// RotateTx3D / RotateTz3D / RotateT2D (fn.cpp:118-166) and
+// ColorFluid::calcTibNorm (colorfluid.cpp:1111-1129), reference arithmetic.
+void rot_cs(double o, double a, double* c, double* s)
+{
+    const double h = std::sqrt(o * o + a * a);
+    *c = 1; *s = 0;
+    if (h != 0) { *c = a / h; *s = o / h; }
+}
+void tib3(const double n[3], double* T)
+{
+    double c, s, tx[9], tz[9];
+    rot_cs(n[0], n[1], &c, &s);
+    const double txv[9] = {c, -s, 0, s, c, 0, 0, 0, 1};
+    std::memcpy(tx, txv, sizeof tx);
+    const double val = std::sqrt(n[0] * n[0] + n[1] * n[1]);
+    rot_cs(val, n[2], &c, &s);
+    const double tzv[9] = {1, 0, 0, 0, c, -s, 0, s, c};
+    std::memcpy(tz, tzv, sizeof tz);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double acc = 0.0;
+            for (int k = 0; k < 3; ++k) acc += tz[3 * i + k] * tx[3 * k + j];
+            T[3 * i + j] = acc;
+        }
+}
+void tib2(const double n[2], double* T)
+{
+    double c, s;
+    rot_cs(n[0], n[1], &c, &s);
+    T[0] = c; T[1] = -s; T[2] = s; T[3] = c;
+}
+
+int setdev(lbf_engine* e)
+{
+    LBF_CK(e, cudaSetDevice(e->cfg.device));
+    return LBF_OK;
+}
+
+Grid grid_of(const lbf_engine* e)
+{
+    Grid g;
+    g.nx = e->nx; g.ny = e->ny; g.nz = e->nz; g.W = e->W;
+    g.nf = e->nf; g.nfp = e->nfp;
+    g.occ = e->occ; g.coord = e->coord;
+    return g;
+}
+
+Macros macros_of(const lbf_engine* e)
+{
+    Macros m;
+    m.rho0 = e->rho0; m.rho1 = e->rho1; m.u = e->u; m.uadj = e->uadj;
+    m.ind = e->ind; m.indadj = e->indadj;
+    return m;
+}
+
+void launch_step(lbf_engine* e, bool pull, int out)
+{
+    const void* fin = e->f[e->cur];
+    void* fout = e->f[e->cur ^ 1];
+    if (e->cfg.model == LBF_MODEL_SCSP) {
+        ScspLaunch a{grid_of(e), e->force, e->sp, fin, fout, macros_of(e), e->err, e->stream};
+        launch_scsp(e->D, (int)e->cfg.storage, e->cfg.collision == LBF_MRT, pull, out, a);
+    } else {
+        ColorWall W{e->angle_id, e->angles, e->tib};
+        ColorLaunch a{grid_of(e), e->force, e->cp, W, fin, fout, e->phi, macros_of(e), e->err, e->stream};
+        launch_color(e->D, (int)e->cfg.storage, (int)e->cfg.collision, pull, out, a);
+    }
+    e->cur ^= 1;
+}
+
+template <class Fn>
+int run_reduce(lbf_engine* e, const Fn& fn, double* out)
+{
+    reduce_pass1<Fn><<<kReduceBlocks, kReduceThreads, 0, e->stream>>>(fn, e->nf, e->partial);
+    reduce_pass2<Fn><<<1, kReduceThreads, 0, e->stream>>>(e->partial, kReduceBlocks, e->red);
+    LBF_CK(e, cudaGetLastError());
+    LBF_CK(e, cudaMemcpyAsync(e->h_red, e->red, Fn::K * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    LBF_CK(e, cudaStreamSynchronize(e->stream));
+    std::memcpy(out, e->h_red, Fn::K * sizeof(double));
+    return LBF_OK;
+}
+
+// Stored populations <-> dense-per-node FP64 ([phase][q][nfp]).
+template <class L, class S>
+__global__ void expand_kernel(const typename S::T* __restrict__ in, double* __restrict__ out,
+                              uint32_t nf, uint32_t nfp, int phases, double rho0)
+{
+    using R = typename S::R;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nf) return;
+    for (int p = 0; p < phases; ++p)
+#pragma unroll
+        for (int q = 0; q < L::Q; ++q) {
+            const size_t j = ((size_t)p * L::Q + q) * nfp + i;
+            const R v = S::load(in + j, q, R(rho0));
+            out[j] = S::shifted ? (L::w36f(q) / 36.0) * rho0 + (double)v : (double)v;
+        }
+}
+
+template <class L, class S>
+__global__ void compress_kernel(const double* __restrict__ in, typename S::T* __restrict__ out,
+                                uint32_t nf, uint32_t nfp, int phases, double rho0)
+{
+    using R = typename S::R;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nf) return;
+    for (int p = 0; p < phases; ++p)
+#pragma unroll
+        for (int q = 0; q < L::Q; ++q) {
+            const size_t j = ((size_t)p * L::Q + q) * nfp + i;
+            const double v = in[j];
+            S::store(out + j, S::shifted ? R(v - (L::w36f(q) / 36.0) * rho0) : R(v), q, R(rho0));
+        }
+}
+
+template <class L>
+void convert(const lbf_engine* e, bool expand, void* f, double* tmp)
+{
+    const unsigned t = 256, b = blocks_for(e->nf, t);
+    if (!b) return;
+    const double r0 = e->cfg.rho[0];
+#define LBF_CONV(S, T)                                                                         \
+    do {                                                                                       \
+        if (expand) expand_kernel<L, S><<<b, t, 0, e->stream>>>((const T*)f, tmp, e->nf, e->nfp, e->phases, r0); \
+        else compress_kernel<L, S><<<b, t, 0, e->stream>>>(tmp, (T*)f, e->nf, e->nfp, e->phases, r0); \
+    } while (0)
+    if (e->cfg.model == LBF_MODEL_COLOR) LBF_CONV(StoreF32Full, float);
+    else if (e->cfg.storage == LBF_STORE_FP16) LBF_CONV(StoreF16<L>, __half);
+    else if (e->cfg.storage == LBF_STORE_BF16) LBF_CONV(StoreBF16<L>, __nv_bfloat16);
+    else LBF_CONV(StoreF32<L>, float);
+#undef LBF_CONV
+}
+
+// Link mask of a voxel from the occupancy map (what the kernels see).
+template <class L>
+__global__ void link_mask_kernel(const Grid g, uint32_t* __restrict__ out, size_t N)
+{
+    const size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= N) return;
+    const int x = (int)(v % g.nx);
+    const int y = (int)((v / g.nx) % g.ny);
+    const int z = (int)(v / ((size_t)g.nx * g.ny));
+    bool fluid;
+    lookup(g, x, y, z, fluid);
+    uint32_t m = 0;
+    if (fluid) {
+#pragma unroll
+        for (int q = 1; q < L::Q; ++q) {
+            bool nf;
+            lookup(g, wrap(x + L::ex(q), g.nx), wrap(y + L::ey(q), g.ny),
+                   L::D == 3 ? wrap(z + L::ez(q), g.nz) : 0, nf);
+            if (!nf) m |= 1u << (q - 1);
+        }
+    }
+    out[v] = m;
+}
+
+int expand_to_host(lbf_engine* e, std::vector<double>& compact)
+{
+    const size_t count = (size_t)e->phases * e->Q * e->nfp;
+    compact.assign(count, 0.0);
+    if (e->cfg.storage == LBF_STORE_FP64) {
+        LBF_CK(e, cudaMemcpyAsync(compact.data(), e->f[e->cur], count * sizeof(double),
+                                  cudaMemcpyDeviceToHost, e->stream));
+        LBF_CK(e, cudaStreamSynchronize(e->stream));
+        return LBF_OK;
+    }
+    double* tmp = nullptr;
+    LBF_CK(e, cudaMalloc(&tmp, count * sizeof(double)));
+    if (e->D == 3) convert<D3Q19>(e, true, e->f[e->cur], tmp);
+    else convert<D2Q9>(e, true, e->f[e->cur], tmp);
+    cudaError_t r = cudaGetLastError();
+    if (r == cudaSuccess) r = cudaMemcpyAsync(compact.data(), tmp, count * sizeof(double), cudaMemcpyDeviceToHost, e->stream);
+    if (r == cudaSuccess) r = cudaStreamSynchronize(e->stream);
+    cudaFree(tmp);
+    if (r != cudaSuccess) return fail(e, LBF_ECUDA, std::string("expand populations: ") + cudaGetErrorString(r));
+    return LBF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t* geometry, lbf_engine** out)
+{
+    if (!out) return fail(nullptr, LBF_EINVAL, "lbf_create: out is NULL");
+    *out = nullptr;
+    if (!cfg || !labels || !geometry) return fail(nullptr, LBF_EINVAL, "lbf_create: NULL argument");
+    const lbf_config& c = *cfg;
+    if (!((c.dims == 2 && c.nz == 1) || c.dims == 3))
+        return fail(nullptr, LBF_EINVAL, "dims must be 2 (with nz = 1) or 3");
+    if (c.nx == 0 || c.ny == 0 || c.nz == 0 || c.nx > 2048 || c.ny > 2048 || c.nz > 1024)
+        return fail(nullptr, LBF_EINVAL, "grid dimensions must be 1..2048 (x, y) and 1..1024 (z)");
+    if (c.model != LBF_MODEL_SCSP && c.model != LBF_MODEL_COLOR)
+        return fail(nullptr, LBF_EINVAL, "unknown fluid model");
+    if (c.collision != LBF_SRT && c.collision != LBF_MRT)
+        return fail(nullptr, LBF_EINVAL, "unknown collision model");
+    if (c.storage > LBF_STORE_FP32) return fail(nullptr, LBF_EINVAL, "unknown storage");
+    if (c.model == LBF_MODEL_COLOR && (c.storage == LBF_STORE_FP16 || c.storage == LBF_STORE_BF16))
+        return fail(nullptr, LBF_EINVAL, "two-phase storage must be FP64 or FP32");
+    const int phases = c.model == LBF_MODEL_COLOR ? 2 : 1;
+    for (int k = 0; k < phases; ++k)
+        if (!std::isfinite(c.tau[k]) || c.tau[k] <= 0.5 || !std::isfinite(c.rho[k]) || c.rho[k] <= 0.0)
+            return fail(nullptr, LBF_EINVAL, "Densities must be positive; relaxation times must exceed 0.5.");
+
+    lbf_engine* e = new (std::nothrow) lbf_engine();
+    if (!e) return fail(nullptr, LBF_ENOMEM, "host allocation failed");
+    e->cfg = c;
+    std::memcpy(e->labels, labels, sizeof e->labels);
+    e->D = (int)c.dims;
+    e->Q = c.dims == 2 ? 9 : 19;
+    e->phases = phases;
+    e->nx = (int)c.nx; e->ny = (int)c.ny; e->nz = (int)c.nz;
+    e->W = (e->nx + 31) / 32;
+    e->N = (size_t)c.nx * c.ny * c.nz;
+    e->elem = c.storage == LBF_STORE_FP64 ? 8 : (c.storage == LBF_STORE_FP32 ? 4 : 2);
+    auto bail = [&](int code, const std::string& m) { lbf_destroy(e); return fail(nullptr, code, m); };
+
+    // Label checks (ValidateSimulation subset, fileprm.cpp:274-294) and the
+    // fluid/solid type sets of buildIb (simulator.cpp:399-415).
+    bool used[256] = {};
+    for (size_t v = 0; v < e->N; ++v) used[geometry[v]] = true;
+    for (int l = 0; l < 256; ++l) {
+        if (!used[l]) continue;
+        const lbf_label& L = labels[l];
+        if (L.type == 0) return bail(LBF_EINVAL, "geometry label " + std::to_string(l) + " is not defined");
+        if (!is_fluid(L.type) && !is_solid(L.type))
+            return bail(LBF_EINVAL, "label " + std::to_string(l) + ": only VD, GV, BB and SD labels are supported");
+        if (is_fluid(L.type) && (L.phase < 0 || L.phase >= phases))
+            return bail(LBF_EINVAL, "Boundary phase is outside the configured fluid model.");
+        if (L.type == LBF_GV && (L.dir <= 0 || L.dir >= e->Q || !std::isfinite(L.value)))
+            return bail(LBF_EINVAL, "Invalid body-force direction or magnitude.");
+    }
+
+    // Occupancy words with prefix counts; fluid nodes in voxel order.
+    const size_t rows = (size_t)e->nz * e->ny;
+    std::vector<uint2> occ(rows * e->W);
+    uint64_t count = 0;
+    for (size_t r = 0; r < rows; ++r)
+        for (int w = 0; w < e->W; ++w) {
+            uint32_t bits = 0;
+            for (int b = 0; b < 32; ++b) {
+                const int x = w * 32 + b;
+                if (x >= e->nx) break;
+                if (is_fluid(labels[geometry[r * e->nx + x]].type)) bits |= 1u << b;
+            }
+            occ[r * e->W + w] = make_uint2(bits, (uint32_t)count);
+            count += (uint64_t)__builtin_popcount(bits);
+        }
+    if (count >= 0xffffffffull) return bail(LBF_EINVAL, "too many fluid nodes");
+    e->nf = (uint32_t)count;
+    e->nfp = (uint32_t)((count + 63) / 64 * 64);
+    if (e->nfp == 0) e->nfp = 64;
+    e->vox.resize(e->nf);
+    std::vector<uint32_t> coord(e->nf);
+    std::vector<uint8_t> nlabel(e->nf), nphase(e->nf);
+    {
+        uint32_t k = 0;
+        for (size_t v = 0; v < e->N; ++v) {
+            const uint8_t l = geometry[v];
+            if (!is_fluid(labels[l].type)) continue;
+            const uint32_t x = (uint32_t)(v % e->nx), y = (uint32_t)((v / e->nx) % e->ny),
+                           z = (uint32_t)(v / ((size_t)e->nx * e->ny));
+            e->vox[k] = (uint32_t)v;
+            coord[k] = x | (y << 11) | (z << 22);
+            nlabel[k] = l;
+            nphase[k] = (uint8_t)labels[l].phase;
+            ++k;
+        }
+    }
+
+    // Body force per label, x/y/z (Simulator::forceForIndex, simulator.cpp:218-228:
+    // Qp[dir] * value, Qp = e / |e|).
+    const double sq = std::sqrt(2) / 2;
+    std::vector<double> lforce(256 * 3, 0.0);
+    for (int l = 0; l < 256; ++l) {
+        const lbf_label& L = labels[l];
+        if (L.type != LBF_GV || L.dir <= 0 || L.dir >= e->Q) continue;
+        int nzc = 0;
+        for (int a = 0; a < 3; ++a) nzc += ecomp(e->D, L.dir, a) != 0;
+        for (int a = 0; a < 3; ++a) {
+            const int ea = ecomp(e->D, L.dir, a);
+            const double qp = nzc == 2 ? ea * sq : (double)ea;
+            lforce[3 * l + a] = qp * L.value;
+        }
+    }
+    bool uniform = true, first = true;
+    double F0[3] = {0, 0, 0};
+    for (int l = 0; l < 256 && uniform; ++l) {
+        if (!used[l] || !is_fluid(labels[l].type)) continue;
+        if (first) { for (int a = 0; a < 3; ++a) F0[a] = lforce[3 * l + a]; first = false; }
+        else for (int a = 0; a < 3; ++a) if (lforce[3 * l + a] != F0[a]) uniform = false;
+    }
+
+    int rc = setdev(e);
+    if (rc) { std::string m = e->last_error; lbf_destroy(e); return fail(nullptr, rc, m); }
+#define LBF_ALLOC(p, n)                                                  \
+    do {                                                                 \
+        int r_ = dalloc(e, &(p), (n));                                   \
+        if (r_) { std::string m_ = e->last_error; lbf_destroy(e); return fail(nullptr, r_, m_); } \
+    } while (0)
+#define LBF_CUDA(call)                                                   \
+    do {                                                                 \
+        cudaError_t r_ = (call);                                         \
+        if (r_ != cudaSuccess) { lbf_destroy(e); return fail(nullptr, LBF_ECUDA, std::string(#call) + ": " + cudaGetErrorString(r_)); } \
+    } while (0)
+    LBF_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+    const size_t fcount = (size_t)phases * e->Q * e->nfp;
+    for (int b = 0; b < 2; ++b) {
+        char* p = nullptr;
+        LBF_ALLOC(p, fcount * e->elem);
+        e->f[b] = p;
+        LBF_CUDA(cudaMemsetAsync(p, 0, fcount * e->elem, e->stream));
+    }
+    LBF_ALLOC(e->occ, occ.size());
+    LBF_ALLOC(e->coord, e->nfp);
+    LBF_ALLOC(e->label_force, 256 * 3);
+    LBF_CUDA(cudaMemcpyAsync(e->occ, occ.data(), occ.size() * sizeof(uint2), cudaMemcpyHostToDevice, e->stream));
+    LBF_CUDA(cudaMemcpyAsync(e->coord, coord.data(), coord.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, e->stream));
+    LBF_CUDA(cudaMemcpyAsync(e->label_force, lforce.data(), lforce.size() * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+    if (!uniform) {
+        LBF_ALLOC(e->node_label, e->nfp);
+        LBF_CUDA(cudaMemcpyAsync(e->node_label, nlabel.data(), nlabel.size(), cudaMemcpyHostToDevice, e->stream));
+    }
+    LBF_ALLOC(e->rho0, e->nfp);
+    LBF_ALLOC(e->u, 3 * (size_t)e->nfp);
+    LBF_ALLOC(e->uprev, 3 * (size_t)e->nfp);
+    LBF_ALLOC(e->uadj, 3 * (size_t)e->nfp);
+    LBF_CUDA(cudaMemsetAsync(e->rho0, 0, e->nfp * sizeof(double), e->stream));
+    LBF_CUDA(cudaMemsetAsync(e->u, 0, 3 * (size_t)e->nfp * sizeof(double), e->stream));
+    LBF_CUDA(cudaMemsetAsync(e->uprev, 0, 3 * (size_t)e->nfp * sizeof(double), e->stream));
+    LBF_CUDA(cudaMemsetAsync(e->uadj, 0, 3 * (size_t)e->nfp * sizeof(double), e->stream));
+    LBF_ALLOC(e->err, 1);
+    LBF_CUDA(cudaMemsetAsync(e->err, 0, sizeof(uint32_t), e->stream));
+    LBF_ALLOC(e->partial, (size_t)kReduceBlocks * kReduceMaxK);
+    LBF_ALLOC(e->red, kReduceMaxK);
+    LBF_CUDA(cudaMallocHost(&e->h_red, kReduceMaxK * sizeof(double)));
+
+    e->force.uniform = uniform ? 1 : 0;
+    e->force.fx = F0[0]; e->force.fy = F0[1]; e->force.fz = F0[2];
+    e->force.label = e->node_label;
+    e->force.label_force = e->label_force;
+
+    if (c.model == LBF_MODEL_SCSP) {
+        e->sp.rho0 = c.rho[0];
+        e->sp.inv_rho0 = 1.0 / c.rho[0];
+        e->sp.omega = 1.0 / c.tau[0];
+        e->sp.mrt = e->D == 3 ? mrt_coef<D3Q19>(c.tau[0]) : mrt_coef<D2Q9>(c.tau[0]);
+    } else {
+        // ColorFluid::initPhi (colorfluid.cpp:1131-1150).
+        double alpha[2];
+        alpha[0] = c.alpha0;
+        alpha[1] = 1 - c.rho[0] / c.rho[1] * (1 - alpha[0]);
+        for (int ph = 0; ph < 2; ++ph)
+            for (int q = 0; q < e->Q; ++q) {
+                double a, b;
+                if (e->Q == 9) { a = (1 - alpha[ph]) / 5; b = (1 - alpha[ph]) / 20; }
+                else { a = (1 - alpha[ph]) / 12; b = (1 - alpha[ph]) / 24; }
+                int nzc = 0;
+                for (int d = 0; d < 3; ++d) nzc += ecomp(e->D, q, d) != 0;
+                e->cp.ai[ph][q] = q == 0 ? alpha[ph] : (nzc == 1 ? a : b);
+            }
+        e->cp.rho_ref[0] = c.rho[0]; e->cp.rho_ref[1] = c.rho[1];
+        e->cp.relax0 = c.tau[0] / 2.0;
+        e->cp.relax1 = c.tau[1] / 2.0;
+        e->cp.uniform_tau = c.tau[0] == c.tau[1];
+        e->cp.mrt = e->D == 3 ? mrt_coef<D3Q19>(c.tau[0]) : mrt_coef<D2Q9>(c.tau[0]);
+        e->cp.ak = 2.25 * c.sigma;
+        e->cp.beta = c.beta;
+
+        // Wall data: mean contact angle per wall node (simulator.cpp:399-430),
+        // deduplicated into a small table, and TibNorm per wall-normal code.
+        static const double pi = 3.1415926535897932384626433832795;
+        std::vector<uint16_t> aid(e->nf, 0);
+        std::map<std::pair<uint64_t, uint64_t>, uint16_t> ids;
+        std::vector<double> ang(2, 0.0);  // id 0 unused
+        for (uint32_t k = 0; k < e->nf; ++k) {
+            const size_t v = e->vox[k];
+            const int x = (int)(v % e->nx), y = (int)((v / e->nx) % e->ny), z = (int)(v / ((size_t)e->nx * e->ny));
+            double ca = 0;
+            int nCA = 0;
+            for (int q = 1; q < e->Q; ++q) {
+                const int ax = (x + ecomp(e->D, q, 0) + e->nx) % e->nx;
+                const int ay = (y + ecomp(e->D, q, 1) + e->ny) % e->ny;
+                const int az = (z + ecomp(e->D, q, 2) + e->nz) % e->nz;
+                const lbf_label& nb = labels[geometry[((size_t)az * e->ny + ay) * e->nx + ax]];
+                if (is_solid(nb.type)) { ca += nb.type == LBF_SD ? nb.value : 0.0; nCA++; }
+            }
+            if (!nCA) continue;
+            ca /= nCA;
+            const double cs = std::cos(ca / 180.0 * pi), sn = std::sin(ca / 180.0 * pi);
+            uint64_t bc, bs;
+            std::memcpy(&bc, &cs, 8); std::memcpy(&bs, &sn, 8);
+            auto key = std::make_pair(bc, bs);
+            auto it = ids.find(key);
+            if (it == ids.end()) {
+                if (ids.size() >= 65535) return bail(LBF_EINVAL, "too many distinct wall contact angles");
+                const uint16_t id = (uint16_t)(ids.size() + 1);
+                it = ids.emplace(key, id).first;
+                ang.push_back(cs); ang.push_back(sn);
+            }
+            aid[k] = it->second;
+        }
+        const int ncodes = e->D == 3 ? normal_codes<D3Q19>() : normal_codes<D2Q9>();
+        const int tsz = e->D == 3 ? 9 : 4;
+        std::vector<double> tib((size_t)ncodes * tsz, 0.0);
+        if (e->D == 3) {
+            for (int a = -5; a <= 5; ++a)
+                for (int b = -5; b <= 5; ++b)
+                    for (int cc = -5; cc <= 5; ++cc) {
+                        const double n[3] = {(double)a, (double)b, (double)cc};
+                        tib3(n, &tib[(size_t)normal_code<D3Q19>(a, b, cc) * 9]);
+                    }
+        } else {
+            for (int a = -3; a <= 3; ++a)
+                for (int b = -3; b <= 3; ++b) {
+                    const double n[2] = {(double)a, (double)b};
+                    tib2(n, &tib[(size_t)normal_code<D2Q9>(a, b, 0) * 4]);
+                }
+        }
+        LBF_ALLOC(e->rho1, e->nfp);
+        LBF_ALLOC(e->ind, e->nfp);
+        LBF_ALLOC(e->indprev, e->nfp);
+        LBF_ALLOC(e->indadj, e->nfp);
+        LBF_ALLOC(e->phi, e->nfp);
+        LBF_ALLOC(e->angle_id, e->nfp);
+        LBF_ALLOC(e->angles, ang.size());
+        LBF_ALLOC(e->tib, tib.size());
+        LBF_ALLOC(e->node_phase, e->nfp);
+        LBF_CUDA(cudaMemsetAsync(e->rho1, 0, e->nfp * sizeof(double), e->stream));
+        LBF_CUDA(cudaMemsetAsync(e->ind, 0, e->nfp * sizeof(double), e->stream));
+        LBF_CUDA(cudaMemsetAsync(e->indprev, 0, e->nfp * sizeof(double), e->stream));
+        LBF_CUDA(cudaMemsetAsync(e->indadj, 0, e->nfp * sizeof(double), e->stream));
+        LBF_CUDA(cudaMemcpyAsync(e->angle_id, aid.data(), aid.size() * sizeof(uint16_t), cudaMemcpyHostToDevice, e->stream));
+        LBF_CUDA(cudaMemcpyAsync(e->angles, ang.data(), ang.size() * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+        LBF_CUDA(cudaMemcpyAsync(e->tib, tib.data(), tib.size() * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+        LBF_CUDA(cudaMemcpyAsync(e->node_phase, nphase.data(), nphase.size(), cudaMemcpyHostToDevice, e->stream));
+        LBF_CUDA(cudaStreamSynchronize(e->stream));
+    }
+    LBF_CUDA(cudaStreamSynchronize(e->stream));
+#undef LBF_ALLOC
+#undef LBF_CUDA
+    *out = e;
+    return LBF_OK;
+}
+
+void lbf_destroy(lbf_engine* e)
+{
+    if (!e) return;
+    cudaSetDevice(e->cfg.device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    void* ptrs[] = {e->f[0], e->f[1], e->occ, e->coord, e->node_label, e->node_phase, e->label_force,
+                    e->rho0, e->rho1, e->u, e->uprev, e->uadj, e->ind, e->indprev, e->indadj,
+                    e->phi, e->angle_id, e->angles, e->tib, e->err, e->partial, e->red};
+    for (void* p : ptrs) if (p) cudaFree(p);
+    if (e->h_red) cudaFreeHost(e->h_red);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+}
+
+int lbf_initialize(lbf_engine* e)
+{
+    if (!e) return fail(e, LBF_EINVAL, "NULL engine");
+    int rc = setdev(e);
+    if (rc) return rc;
+    const Grid g = grid_of(e);
+    if (e->cfg.model == LBF_MODEL_SCSP)
+        launch_scsp_init(e->D, (int)e->cfg.storage, g, e->force, e->cfg.rho[0], e->f[e->cur], e->stream);
+    else
+        launch_color_init(e->D, (int)e->cfg.storage, g, e->force, e->cp, e->node_phase, e->f[e->cur], e->stream);
+    launch_step(e, false, kOutMacros | kOutAdjacent);
+    LBF_CK(e, cudaGetLastError());
+    e->initialized = true;
+    return LBF_OK;
+}
+
+int lbf_step(lbf_engine* e, uint32_t nsteps, uint32_t flags)
+{
+    if (!e) return fail(e, LBF_EINVAL, "NULL engine");
+    if (!e->initialized) return fail(e, LBF_ESTATE, "lbf_step before lbf_initialize or lbf_set_populations");
+    int rc = setdev(e);
+    if (rc) return rc;
+    const int out = (flags & LBF_STEP_MACROS ? kOutMacros : 0) | (flags & LBF_STEP_ADJACENT ? kOutAdjacent : 0);
+    for (uint32_t s = 0; s < nsteps; ++s) launch_step(e, true, s + 1 == nsteps ? out : 0);
+    LBF_CK(e, cudaGetLastError());
+    return LBF_OK;
+}
+
+int lbf_get_populations(lbf_engine* e, double* host, size_t n)
+{
+    if (!e || !host) return fail(e, LBF_EINVAL, "NULL argument");
+    const size_t need = (size_t)e->phases * e->Q * e->N;
+    if (n != need) return fail(e, LBF_EINVAL, "population buffer must hold phases*Q*N doubles");
+    int rc = setdev(e);
+    if (rc) return rc;
+    std::vector<double> compact;
+    rc = expand_to_host(e, compact);
+    if (rc) return rc;
+    std::memset(host, 0, n * sizeof(double));
+    for (int p = 0; p < e->phases; ++p)
+        for (int q = 0; q < e->Q; ++q) {
+            const double* src = compact.data() + ((size_t)p * e->Q + q) * e->nfp;
+            double* dst = host + ((size_t)p * e->Q + q) * e->N;
+            for (uint32_t k = 0; k < e->nf; ++k) dst[e->vox[k]] = src[k];
+        }
+    return LBF_OK;
+}
+
+int lbf_set_populations(lbf_engine* e, const double* host, size_t n)
+{
+    if (!e || !host) return fail(e, LBF_EINVAL, "NULL argument");
+    const size_t need = (size_t)e->phases * e->Q * e->N;
+    if (n != need) return fail(e, LBF_EINVAL, "population buffer must hold phases*Q*N doubles");
+    int rc = setdev(e);
+    if (rc) return rc;
+    const size_t count = (size_t)e->phases * e->Q * e->nfp;
+    std::vector<double> compact(count, 0.0);
+    for (int p = 0; p < e->phases; ++p)
+        for (int q = 0; q < e->Q; ++q) {
+            const double* src = host + ((size_t)p * e->Q + q) * e->N;
+            double* dst = compact.data() + ((size_t)p * e->Q + q) * e->nfp;
+            for (uint32_t k = 0; k < e->nf; ++k) dst[k] = src[e->vox[k]];
+        }
+    if (e->cfg.storage == LBF_STORE_FP64) {
+        LBF_CK(e, cudaMemcpyAsync(e->f[e->cur], compact.data(), count * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+        LBF_CK(e, cudaStreamSynchronize(e->stream));
+    } else {
+        double* tmp = nullptr;
+        LBF_CK(e, cudaMalloc(&tmp, count * sizeof(double)));
+        cudaError_t r = cudaMemcpyAsync(tmp, compact.data(), count * sizeof(double), cudaMemcpyHostToDevice, e->stream);
+        if (r == cudaSuccess) {
+            if (e->D == 3) convert<D3Q19>(e, false, e->f[e->cur], tmp);
+            else convert<D2Q9>(e, false, e->f[e->cur], tmp);
+            r = cudaGetLastError();
+        }
+        if (r == cudaSuccess) r = cudaStreamSynchronize(e->stream);
+        cudaFree(tmp);
+        if (r != cudaSuccess) return fail(e, LBF_ECUDA, std::string("set populations: ") + cudaGetErrorString(r));
+    }
+    e->initialized = true;
+    return LBF_OK;
+}
+
+int lbf_get_macros(lbf_engine* e, double* rho0, double* rho1, double* u)
+{
+    if (!e) return fail(e, LBF_EINVAL, "NULL engine");
+    int rc = setdev(e);
+    if (rc) return rc;
+    std::vector<double> buf((size_t)e->nfp * 3);
+    auto scatter = [&](const double* dsrc, double* dst, int comps) -> int {
+        LBF_CK(e, cudaMemcpyAsync(buf.data(), dsrc, (size_t)comps * e->nfp * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+        LBF_CK(e, cudaStreamSynchronize(e->stream));
+        std::memset(dst, 0, (size_t)comps * e->N * sizeof(double));
+        for (int c = 0; c < comps; ++c)
+            for (uint32_t k = 0; k < e->nf; ++k) dst[(size_t)c * e->N + e->vox[k]] = buf[(size_t)c * e->nfp + k];
+        return LBF_OK;
+    };
+    if (rho0 && (rc = scatter(e->rho0, rho0, 1))) return rc;
+    if (rho1) {
+        if (e->rho1) { if ((rc = scatter(e->rho1, rho1, 1))) return rc; }
+        else std::memset(rho1, 0, e->N * sizeof(double));
+    }
+    if (u && (rc = scatter(e->u, u, 3))) return rc;
+    return LBF_OK;
+}
+
+int lbf_convergence(lbf_engine* e, int first, double out[6])
+{
+    if (!e || !out) return fail(e, LBF_EINVAL, "NULL argument");
+    int rc = setdev(e);
+    if (rc) return rc;
+    for (int k = 0; k < 6; ++k) out[k] = 0.0;
+    const bool color = e->cfg.model == LBF_MODEL_COLOR;
+    if (!first) {
+        ConvergenceFn fn{e->u, e->uprev, e->uadj, e->ind, e->indprev, e->indadj, e->nfp, color ? 1 : 0};
+        double r[ConvergenceFn::K];
+        if ((rc = run_reduce(e, fn, r))) return rc;
+        for (int k = 0; k < ConvergenceFn::K; ++k) out[k] = r[k];
+    }
+    LBF_CK(e, cudaMemcpyAsync(e->uprev, e->u, 3 * (size_t)e->nfp * sizeof(double), cudaMemcpyDeviceToDevice, e->stream));
+    if (color)
+        LBF_CK(e, cudaMemcpyAsync(e->indprev, e->ind, (size_t)e->nfp * sizeof(double), cudaMemcpyDeviceToDevice, e->stream));
+    LBF_CK(e, cudaStreamSynchronize(e->stream));
+    return LBF_OK;
+}
+
+int lbf_report_sums(lbf_engine* e, uint32_t axis, uint32_t lo, uint32_t hi, double out[10])
+{
+    if (!e || !out || axis > 2) return fail(e, LBF_EINVAL, "invalid argument");
+    int rc = setdev(e);
+    if (rc) return rc;
+    ReportFn fn{e->coord, e->u, e->rho0, e->rho1, e->nfp, (int)axis, (int)lo, (int)hi};
+    return run_reduce(e, fn, out);
+}
+
+int lbf_flux_sums(lbf_engine* e, double out[9])
+{
+    if (!e || !out) return fail(e, LBF_EINVAL, "NULL argument");
+    int rc = setdev(e);
+    if (rc) return rc;
+    FluxFn fn{e->u, e->rho0, e->rho1, e->nfp};
+    return run_reduce(e, fn, out);
+}
+
+int lbf_link_mask(lbf_engine* e, uint32_t* host, size_t n)
+{
+    if (!e || !host || n != e->N) return fail(e, LBF_EINVAL, "mask buffer must hold nx*ny*nz entries");
+    int rc = setdev(e);
+    if (rc) return rc;
+    uint32_t* d = nullptr;
+    LBF_CK(e, cudaMalloc(&d, e->N * sizeof(uint32_t)));
+    const unsigned t = 256;
+    const unsigned b = (unsigned)((e->N + t - 1) / t);
+    if (e->D == 3) link_mask_kernel<D3Q19><<<b, t, 0, e->stream>>>(grid_of(e), d, e->N);
+    else link_mask_kernel<D2Q9><<<b, t, 0, e->stream>>>(grid_of(e), d, e->N);
+    cudaError_t r = cudaGetLastError();
+    if (r == cudaSuccess) r = cudaMemcpyAsync(host, d, e->N * sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream);
+    if (r == cudaSuccess) r = cudaStreamSynchronize(e->stream);
+    cudaFree(d);
+    if (r != cudaSuccess) return fail(e, LBF_ECUDA, std::string("link mask: ") + cudaGetErrorString(r));
+    return LBF_OK;
+}
+
+int lbf_status(lbf_engine* e, uint32_t* bits)
+{
+    if (!e || !bits) return fail(e, LBF_EINVAL, "NULL argument");
+    int rc = setdev(e);
+    if (rc) return rc;
+    LBF_CK(e, cudaStreamSynchronize(e->stream));
+    LBF_CK(e, cudaMemcpy(bits, e->err, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    return LBF_OK;
+}
+
+int lbf_synchronize(lbf_engine* e)
+{
+    if (!e) return fail(e, LBF_EINVAL, "NULL engine");
+    int rc = setdev(e);
+    if (rc) return rc;
+    LBF_CK(e, cudaStreamSynchronize(e->stream));
+    return LBF_OK;
+}
+
+uint64_t lbf_fluid_nodes(const lbf_engine* e) { return e ? e->nf : 0; }
+void* lbf_stream(const lbf_engine* e) { return e ? (void*)e->stream : nullptr; }
+uint64_t lbf_device_bytes(const lbf_engine* e) { return e ? e->bytes : 0; }
+
+const char* lbf_last_error(const lbf_engine* e)
+{
+    return e ? e->last_error.c_str() : g_create_error.c_str();
+}
+
+}  // extern "C"

@@ -1,0 +1,44 @@
+// Internal interfaces between the engine's translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "kernels.cuh"
+#include "color.cuh"
+
+namespace lbf {
+
+struct ScspLaunch {
+    Grid g;
+    Force F;
+    ScspParams P;
+    const void* fin;
+    void* fout;
+    Macros mo;
+    uint32_t* err;
+    cudaStream_t stream;
+};
+
+struct ColorLaunch {
+    Grid g;
+    Force F;
+    ColorParams P;
+    ColorWall W;
+    const void* fin;   // [2][Q][nfp]
+    void* fout;
+    double* phi;       // [nfp] phase field of this step (written by pass 1)
+    Macros mo;
+    uint32_t* err;
+    cudaStream_t stream;
+};
+
+// storage: LBF_STORE_* value; dims: 2 or 3.
+void launch_scsp(int dims, int storage, bool mrt, bool pull, int out, const ScspLaunch& a);
+void launch_scsp_init(int dims, int storage, const Grid& g, const Force& F, double rho0,
+                      void* f, cudaStream_t s);
+void launch_color(int dims, int storage, int collision, bool pull, int out, const ColorLaunch& a);
+void launch_color_init(int dims, int storage, const Grid& g, const Force& F, const ColorParams& P,
+                       const uint8_t* phase, void* f, cudaStream_t s);
+
+inline unsigned blocks_for(uint32_t n, unsigned threads) { return (n + threads - 1) / threads; }
+
+}  // namespace lbf

@@ -1,0 +1,154 @@
+"""Small solver cases shared by the golden-fixture script and the tests.
+
+Each case is a dict with the geometry (uint8, shaped (nz, ny, nx) or (ny, nx)),
+the label table, the model parameters and the step count.  The geometries
+follow the reference's own test inputs: the channel of examples/generate.py,
+the uniform body-force boxes of scripts/benchmarks.py:176-188, the drop of
+scripts/ci_smoke.py:50-54, plus small porous media made with the
+Gaussian-filtered-noise recipe (lbflow_b200.geometry).
+"""
+import numpy as np
+
+
+def _labels_channel(force):
+    return {75: ('GV', force, 1, 0), 255: ('SD', 90.0, 0, 0)}
+
+
+def channel_config1():
+    """Config 1: 8x10x4 channel, SD planes at y=0 and y=9, SRT tau=0.8, g_x=1e-6, 20000 steps."""
+    nx, ny, nz = 8, 10, 4
+    g = np.full((nz, ny, nx), 75, np.uint8)
+    g[:, 0, :] = 255
+    g[:, ny - 1, :] = 255
+    return dict(name='channel-config1', geometry=g, labels=_labels_channel(1e-6), model='scsp',
+                collision='SRT', tau=(0.8,), rho=(1.0,), steps=20000, write=20000)
+
+
+def channel_mrt():
+    """examples/generate.py channel: MRT tau=1, 1000 steps."""
+    c = channel_config1()
+    c.update(name='channel-mrt', collision='MRT', tau=(1.0,), steps=1000, write=1000)
+    return c
+
+
+def force_cases():
+    """Uniform periodic GV boxes (scripts/benchmarks.py:176-188): u_x = 1e-4 after 100 steps."""
+    out = []
+    for model in ('scsp', 'color'):
+        for ndim in (2, 3):
+            for eq in ('SRT', 'MRT'):
+                for tau in (0.6, 1.4):
+                    nx, ny, nz = 8, 6, (1 if ndim == 2 else 4)
+                    shape = (ny, nx) if ndim == 2 else (nz, ny, nx)
+                    g = np.full(shape, 75, np.uint8)
+                    ph = 1 if model == 'color' else 0
+                    out.append(dict(name=f'force-{model}-d{ndim}-{eq}-tau{tau}', geometry=g,
+                                    labels={75: ('GV', 1e-6, 1, ph)}, model=model, collision=eq,
+                                    tau=(0.8, tau) if model == 'color' else (tau,),
+                                    rho=(1.0, 1.0) if model == 'color' else (1.0,),
+                                    alpha0=4 / 9 if ndim == 2 else 1 / 3, sigma=0.005, beta=0.7,
+                                    steps=100, write=50))
+    return out
+
+
+def drop_3d():
+    """scripts/ci_smoke.py drop: 12^3 color D3Q19 MRT, 40 steps."""
+    n = 12
+    z, y, x = np.mgrid[0:n, 0:n, 0:n]
+    g = np.where((x - 5.5) ** 2 + (y - 5.5) ** 2 + (z - 5.5) ** 2 <= 9, 100, 0).astype(np.uint8)
+    return dict(name='drop-3d', geometry=g, labels={0: ('VD', 0, 0, 0), 100: ('VD', 0, 0, 1)},
+                model='color', collision='MRT', tau=(1.0, 1.0), rho=(1.0, 1.0), alpha0=1 / 3,
+                sigma=0.005, beta=0.7, steps=40, write=20)
+
+
+def wall_color_3d(tau1=0.7, collision='MRT'):
+    """Two-phase channel with an obstacle, SD walls at 60 degrees, GV in x per phase."""
+    nx, ny, nz = 12, 10, 8
+    g = np.full((nz, ny, nx), 75, np.uint8)
+    g[:, 0, :] = 255
+    g[:, -1, :] = 255
+    g[3:5, 4:6, 3:6] = 255
+    blk = g[2:6, 2:8, 7:11]
+    blk[blk == 75] = 76
+    return dict(name=f'wall-color-3d-{collision}-{tau1}', geometry=g,
+                labels={75: ('GV', 2e-6, 1, 0), 76: ('GV', 2e-6, 1, 1), 255: ('SD', 60.0, 0, 0)},
+                model='color', collision=collision, tau=(1.0, tau1), rho=(1.0, 1.0), alpha0=1 / 3,
+                sigma=1e-3, beta=0.7, steps=200, write=200)
+
+
+def wall_color_2d(collision='MRT'):
+    """D2Q9 drop between SD walls (45 degrees) with a BB block."""
+    nx, ny = 20, 16
+    g = np.zeros((ny, nx), np.uint8)
+    g[0, :] = 255
+    g[-1, :] = 255
+    g[6:9, 12:15] = 254
+    yy, xx = np.mgrid[0:ny, 0:nx]
+    g[((xx - 6) ** 2 + (yy - 7) ** 2 <= 9) & (g == 0)] = 100
+    return dict(name=f'wall-color-2d-{collision}', geometry=g,
+                labels={0: ('VD', 0, 0, 0), 100: ('VD', 0, 0, 1), 255: ('SD', 45.0, 0, 0),
+                        254: ('BB', 0.0, 0, 0)},
+                model='color', collision=collision, tau=(1.0, 0.8), rho=(1.0, 1.0), alpha0=4 / 9,
+                sigma=5e-3, beta=0.7, steps=300, write=300)
+
+
+def porous_scsp(collision='MRT', n=(16, 16, 12), seed=7):
+    """Small Gaussian-filtered porous medium, single phase, GV in x."""
+    from lbflow_b200.geometry import porous_medium
+    nx, ny, nz = n
+    fluid = porous_medium((nz, ny, nx), sigma=2.0, porosity=0.35, seed=seed)
+    g = np.where(fluid, 75, 255).astype(np.uint8)
+    return dict(name=f'porous-scsp-{collision}', geometry=g,
+                labels={75: ('GV', 1e-5, 1, 0), 255: ('SD', 90.0, 0, 0)},
+                model='scsp', collision=collision, tau=(1.0,), rho=(1.0,), steps=300, write=300)
+
+
+def porous_scsp_2d(collision='MRT'):
+    from lbflow_b200.geometry import porous_medium
+    fluid = porous_medium((1, 40, 48), sigma=2.0, porosity=0.5, seed=3)[0]
+    g = np.where(fluid, 75, 255).astype(np.uint8)
+    return dict(name=f'porous-scsp-2d-{collision}', geometry=g,
+                labels={75: ('GV', 1e-5, 1, 0), 255: ('BB', 0.0, 0, 0)},
+                model='scsp', collision=collision, tau=(0.9,), rho=(1.0,), steps=400, write=400)
+
+
+def golden_cases():
+    """The cases whose reference outputs are committed under tests/golden/."""
+    return ([channel_config1(), channel_mrt(), drop_3d(), wall_color_3d(0.7, 'MRT'),
+             wall_color_3d(1.0, 'SRT'), wall_color_2d('MRT'), wall_color_2d('SRT'),
+             porous_scsp('MRT'), porous_scsp('SRT'), porous_scsp_2d('MRT')] + force_cases())
+
+
+def prm_text(case, grid_file='geometry.raw', out='field', report_dir=0):
+    """An input.prm for the case, in the form scripts/benchmarks.py writes (:73-101)."""
+    g = case['geometry']
+    ndim = 2 if g.ndim == 2 else 3
+    if ndim == 2:
+        ny, nx = g.shape
+        dims = f'{ny} {nx}'
+    else:
+        nz, ny, nx = g.shape
+        dims = f'{nz} {ny} {nx}'
+    color = case['model'] == 'color'
+    lines = [
+        f'gridFile "{grid_file}";', f'dimension {dims};', f'directions {9 if ndim == 2 else 19};',
+        'fileType "uint8";', 'latticeLen 1;', 'startTime 0;', f'endTime {case["steps"]};',
+        f'writeInterval {case["write"]};', f'reportInterval {case.get("report", case["write"])};',
+        f'restartInterval {case.get("restart", case["steps"])};',
+        f'stopError {case.get("stop_error", 1e-8)};', f'outPath "{out}";', 'logPath ".";',
+        f'reportDir {report_dir};', f'reportSlice 1 {nx - 2};',
+        f'fluidModel "{case["model"]}";', f'equilModel "{case["collision"]}";',
+        'rexlationTime ' + ' '.join(format(t, '.17g') for t in case['tau']) + ';',
+        'latticeSpeed 1;', f'alpha0 {format(case.get("alpha0", 1 / 3), ".17g")};',
+        'density ' + ' '.join(map(str, case['rho'])) + ';', 'contactAngle 90;',
+        f'surfaceTension {case.get("sigma", 0.005)};', f'interfaceThickness {case.get("beta", 0.7)};',
+        'wallGradient "legacy";', 'viscosityInterpolation "arithmetic";',
+    ]
+    for k, (t, v, d, ph) in sorted(case['labels'].items()):
+        val = 'N/A' if t in ('VD', 'BB') else format(v, '.17g') if t == 'GV' else format(v, 'g')
+        dr = str(d) if t == 'GV' else 'N/A'
+        p = str(ph) if t in ('VD', 'GV') else 'N/A'
+        lines.append(f'{k} "{t}" "{val}" "{dr}" "{p}"')
+    if not color:
+        pass
+    return '\n'.join(lines) + '\n'

@@ -1,0 +1,64 @@
+"""The C-ABI library: loads, exports what include/lbflow.h declares, validates input (no GPU needed)."""
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared_functions():
+    text = (ROOT / 'include' / 'lbflow.h').read_text()
+    return sorted(set(re.findall(r'\b(lbf_[a-z_]+)\s*\(', text)))
+
+
+def test_library_exports_every_declared_symbol():
+    import lbflow_b200
+    lib = lbflow_b200.library()
+    names = declared_functions()
+    assert len(names) >= 15
+    for n in names:
+        assert hasattr(lib, n), n
+
+
+def _create(**over):
+    import lbflow_b200 as L
+    lib = L.library()
+    cfg = dict(dims=3, nx=4, ny=4, nz=4, model=0, collision=1, storage=0, device=0)
+    cfg.update(over)
+    c = L._Config(cfg['dims'], cfg['nx'], cfg['ny'], cfg['nz'], cfg['model'], cfg['collision'],
+                  cfg['storage'], cfg['device'], (ctypes.c_double * 2)(*over.get('tau', (1.0, 1.0))),
+                  (ctypes.c_double * 2)(1.0, 1.0), 1 / 3, 0.0, 0.0)
+    labels = L.make_labels(over.get('labels', {0: ('VD', 0, 0, 0)}))
+    geom = over.get('geometry', np.zeros(64, np.uint8))
+    h = ctypes.c_void_p()
+    rc = lib.lbf_create(ctypes.byref(c), labels, geom.tobytes(), ctypes.byref(h))
+    return rc, lib.lbf_last_error(None).decode()
+
+
+@pytest.mark.parametrize('over,msg', [
+    (dict(dims=4), 'dims'),
+    (dict(nx=4096), 'grid dimensions'),
+    (dict(model=7), 'fluid model'),
+    (dict(collision=5), 'collision'),
+    (dict(tau=(0.5, 1.0)), 'relaxation times must exceed 0.5'),
+    (dict(labels={}), 'not defined'),
+    (dict(labels={0: ('PB', 1.0, 1, 0)}), 'only VD, GV, BB and SD'),
+    (dict(labels={0: ('GV', 1e-6, 19, 0)}), 'body-force direction'),
+    (dict(labels={0: ('VD', 0, 0, 1)}), 'phase'),
+    (dict(model=1, storage=1), 'two-phase storage'),
+])
+def test_create_rejects_invalid_input(over, msg):
+    rc, err = _create(**over)
+    assert rc == -1
+    assert msg in err
+
+
+def test_null_arguments():
+    import lbflow_b200 as L
+    lib = L.library()
+    assert lib.lbf_create(None, None, None, None) == -1
+    assert lib.lbf_step(None, 1, 0) == -1
+    assert lib.lbf_fluid_nodes(None) == 0
