@@ -55,7 +55,8 @@ def profile_traffic(storage):
         return None
     for line in p.read_text().splitlines():
         if line.startswith('traffic_bytes_per_launch:'):
-            return float(line.split(':', 1)[1])
+            v = line.split(':', 1)[1].strip()
+            return None if v in ('', 'null') else float(v)
     return None
 
 

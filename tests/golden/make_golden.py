@@ -65,6 +65,72 @@ def main():
                                    total_voxels=timing['total_voxels'])
         print(case['name'], f.size, sorted(vti))
     (HERE / 'index.json').write_text(json.dumps(index, indent=1, sort_keys=True) + '\n')
+    cli_contracts(exe)
+
+
+def run_ref(exe, case, prm=None, extra=None):
+    """Run the reference on a case; return (exit code, stdout, {file: bytes})."""
+    with tempfile.TemporaryDirectory() as d:
+        d = Path(d)
+        case['geometry'].tofile(d / 'geometry.raw')
+        (d / 'input.prm').write_text(prm if prm is not None else prm_text(case))
+        if extra:
+            extra(d)
+        r = subprocess.run([str(exe), 'input.prm'], cwd=d, capture_output=True, text=True)
+        files = {p.name: p.read_bytes() for p in d.iterdir() if p.name.startswith('field')}
+        return r.returncode, r.stdout, files
+
+
+def cli_contracts(exe):
+    """Reference behaviour of the command line: error messages of invalid
+    inputs, VTI headers, checkpoint sidecars and report lines."""
+    from cases import force_cases, channel_mrt, wall_color_2d, porous_scsp, wall_color_3d
+    import re
+    out = {'errors': {}, 'vti_header': {}, 'meta': {}, 'reports': {}}
+    base = force_cases()[7]          # force-scsp-d3-MRT-tau1.4
+    cbase = force_cases()[-1]        # force-color-d3-MRT-tau1.4
+    text = prm_text(base)
+    ctext = prm_text(cbase)
+    def sub(t, key, val):
+        return re.sub(rf'^{key} .*;$', f'{key} {val};', t, flags=re.M)
+    invalid = {
+        'zero-write': (base, sub(text, 'writeInterval', '0')),
+        'invalid-tau': (base, sub(text, 'rexlationTime', '0.5')),
+        'invalid-speed': (base, sub(text, 'latticeSpeed', '2')),
+        'invalid-alpha': (cbase, sub(ctext, 'alpha0', '1.1')),
+        'invalid-color-tau': (cbase, sub(ctext, 'rexlationTime', '.5 .5')),
+        'tau-count': (base, sub(text, 'rexlationTime', '1 1')),
+        'bad-model': (base, sub(text, 'fluidModel', '"foo"')),
+        'shanchen': (base, sub(text, 'fluidModel', '"shanchen"')),
+        'bad-equil': (base, sub(text, 'equilModel', '"BGK"')),
+        'bad-directions': (base, sub(text, 'directions', '15')),
+        'short-geometry': (base, sub(text, 'dimension', '5 6 8')),
+        'missing-geometry': (base, sub(text, 'gridFile', '"nothere.raw"')),
+        'undefined-label': (base, text.replace('75 "GV"', '76 "GV"')),
+        'bad-label-type': (base, text.replace('75 "GV"', '75 "XX"')),
+        'bad-force-dir': (base, text.replace('"1" "0"', '"0" "0"')),
+        'missing-key': (base, text.replace('stopError 1e-08;', '')),
+        'report-slice': (base, sub(sub(text, 'reportDir', '3'), 'reportSlice', '1 6')),
+        'report-dir': (base, sub(text, 'reportDir', '19')),
+        'sd-angle': (channel_mrt(), prm_text(channel_mrt()).replace('"SD" "90"', '"SD" "190"')),
+    }
+    for name, (case, prm) in invalid.items():
+        code, stdout, _ = run_ref(exe, case, prm)
+        assert code != 0 and 'Simulation finished!' not in stdout, name
+        msg = [l for l in stdout.splitlines() if 'Failed to excute: ' in l][-1].split('Failed to excute: ', 1)[1]
+        out['errors'][name] = dict(prm=prm, message=msg, geometry_case=case['name'])
+    for case in (channel_mrt(), wall_color_2d('MRT')):
+        code, stdout, files = run_ref(exe, case)
+        vti = files[f'field.{case["steps"]:010d}.vti']
+        out['vti_header'][case['name']] = vti[:vti.index(b'>_') + 2].decode()
+        out['meta'][case['name']] = files[f'field.{case["steps"]:010d}.rst.meta'].decode()
+    for case, rdir in ((dict(porous_scsp('MRT'), report=50, steps=300), 1),
+                       (dict(wall_color_3d(0.7, 'MRT'), report=50, steps=200), 1)):
+        code, stdout, _ = run_ref(exe, case, prm_text(case, report_dir=rdir))
+        lines = [l for l in stdout.splitlines() if l.startswith(' - ') or l.startswith('Step ')]
+        out['reports'][case['name']] = dict(report_dir=rdir, report=case['report'], steps=case['steps'],
+                                            lines=lines)
+    (HERE / 'cli_contracts.json').write_text(json.dumps(out, indent=1, sort_keys=True) + '\n')
 
 
 if __name__ == '__main__':
