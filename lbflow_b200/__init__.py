@@ -91,6 +91,7 @@ def library():
             'lbf_last_error': (ctypes.c_char_p, [P]),
             'lbf_synchronize': (I, [P]),
             'lbf_stream': (P, [P]),
+            'lbf_flux_sums_noalloc': (I, [P, P, P, U32, U32, P, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)

@@ -305,6 +305,10 @@ int expand_to_host(lbf_engine* e, std::vector<double>& compact)
 
 }  // namespace
 
+namespace lbf {
+void set_global_error(const std::string& msg) { g_create_error = msg; }
+}  // namespace lbf
+
 extern "C" {
 
 int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t* geometry, lbf_engine** out)

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <string>
 #include "kernels.cuh"
 #include "color.cuh"
 
@@ -38,6 +39,9 @@ void launch_scsp_init(int dims, int storage, const Grid& g, const Force& F, doub
 void launch_color(int dims, int storage, int collision, bool pull, int out, const ColorLaunch& a);
 void launch_color_init(int dims, int storage, const Grid& g, const Force& F, const ColorParams& P,
                        const uint8_t* phase, void* f, cudaStream_t s);
+
+// Message returned by lbf_last_error(NULL) (calls without an engine).
+void set_global_error(const std::string& msg);
 
 inline unsigned blocks_for(uint32_t n, unsigned threads) { return (n + threads - 1) / threads; }
 
