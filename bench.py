@@ -35,8 +35,9 @@ sys.path.insert(0, str(ROOT))
 METRIC = 'D3Q19 MRT fluid MLUPS (256^3 porous cube, porosity 0.22)'
 # Algorithmic bytes per fluid-node update: read + write Q populations, plus
 # the 4-byte link information (2*Q*s + 4).
-ALG_BYTES = {'fp64': 2 * 19 * 8 + 4, 'fp32': 2 * 19 * 4 + 4, 'fp16': 2 * 19 * 2 + 4, 'bf16': 2 * 19 * 2 + 4}
-ELEM = {'fp64': 8, 'fp32': 4, 'fp16': 2, 'bf16': 2}
+ALG_BYTES = {'fp64': 2 * 19 * 8 + 4, 'fp32': 2 * 19 * 4 + 4, 'fp16': 2 * 19 * 2 + 4, 'bf16': 2 * 19 * 2 + 4,
+             'bfp16': 2 * 19 * 2 + 2 + 4}
+ELEM = {'fp64': 8, 'fp32': 4, 'fp16': 2, 'bf16': 2, 'bfp16': 2}
 REF_SAMPLE = dict(n=64, sigma=3.0, porosity=0.22, seed=0)
 
 
@@ -210,16 +211,22 @@ def main():
     ap.add_argument('--steps', type=int, default=5000)
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='ours', choices=('ours', 'reference'))
-    ap.add_argument('--storage', default='fp64', choices=('fp64', 'fp32', 'fp16', 'bf16'))
+    ap.add_argument('--storage', default='fp64', choices=('fp64', 'fp32', 'fp16', 'bf16', 'bfp16'))
     ap.add_argument('--collision', default='MRT', choices=('MRT', 'SRT'))
     ap.add_argument('--size', type=int, default=256)
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true')
+    ap.add_argument('--mode', default='mlups', choices=('mlups', 'ttp'),
+                    help='mlups: the throughput line; ttp: time to permeability, plain FP64 vs reduced storage')
+    ap.add_argument('--storages', default='fp64,bfp16,fp16,fp32')
+    ap.add_argument('--max-steps', type=int, default=400000)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == 'reference':
         return run_reference_arm(args)
+    if args.mode == 'ttp':
+        return time_to_permeability(args)
 
     import torch
     import torch.distributed as dist
@@ -306,6 +313,45 @@ def main():
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
+    return 0
+
+
+def time_to_permeability(args):
+    """Wall time to LBFlow's convergence criterion (report every 1000 steps,
+    relative velocity change < 1e-6 three times in a row) for the plain FP64
+    path and each reduced-precision storage, with K = nu <u_x> / g and its
+    error against the FP64 result."""
+    import torch
+    from lbflow_b200 import Engine
+    from lbflow_b200.permeability import converge, time_to_band
+    torch.cuda.set_device(0)
+    geometry = make_geometry(args.size, 3.0, 0.22, seed=0)
+    runs = {}
+    hist = {}
+    for storage in args.storages.split(','):
+        eng = Engine(geometry, LABELS, model='scsp', collision=args.collision, tau=(1.0,), rho=(1.0,),
+                     storage=storage)
+        r = converge(eng, 1.0, 1e-5, report=1000, tol=1e-6, max_steps=args.max_steps)
+        hist[storage] = r['history']
+        runs[storage] = dict(steps=r['steps'], seconds=r['seconds'], K=r['K'], converged=r['converged'],
+                             fluid_nodes=eng.fluid_nodes,
+                             mlups=eng.fluid_nodes * r['steps'] / r['seconds'] / 1e6)
+        eng.close()
+    base = runs.get('fp64')
+    for k, v in runs.items():
+        if base:
+            v['K_rel_error_vs_fp64'] = abs(v['K'] - base['K']) / abs(base['K'])
+            v['speedup_vs_fp64'] = base['seconds'] / v['seconds']
+            band = time_to_band(hist[k], base['K'], 1e-3)
+            v['to_1e-3_band'] = dict(steps=band[0], seconds=band[1]) if band else None
+    if base and runs['fp64'].get('to_1e-3_band'):
+        b0 = runs['fp64']['to_1e-3_band']['seconds']
+        for k, v in runs.items():
+            if v.get('to_1e-3_band'):
+                v['to_1e-3_band']['speedup_vs_fp64'] = b0 / v['to_1e-3_band']['seconds']
+    print(json.dumps(dict(metric='time to permeability (1e-6 convergence, K within 1e-3 of FP64)',
+                          workload=f'D3Q19 {args.collision} porous cube {args.size}^3, porosity 0.22, sigma 3, '
+                                   f'tau 1, g_x 1e-5', runs=runs)))
     return 0
 
 

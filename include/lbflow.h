@@ -52,8 +52,11 @@ enum { LBF_MODEL_SCSP = 0, LBF_MODEL_COLOR = 1 };
 enum { LBF_SRT = 0, LBF_MRT = 1 };
 /* Population storage.  FP64 is the plain path (FP64 arithmetic).  The others
  * store shifted deviations f_q - w_q*rho0, scaled per direction, and collide
- * in FP32; reductions stay FP64. */
-enum { LBF_STORE_FP64 = 0, LBF_STORE_FP16 = 1, LBF_STORE_BF16 = 2, LBF_STORE_FP32 = 3 };
+ * in FP32; reductions stay FP64.  BFP16 stores (f_q - w_q*rho0)/w_q as int16
+ * mantissas with one power-of-two exponent byte per node (block floating
+ * point); single phase only, like FP16 and BF16. */
+enum { LBF_STORE_FP64 = 0, LBF_STORE_FP16 = 1, LBF_STORE_BF16 = 2, LBF_STORE_FP32 = 3,
+       LBF_STORE_BFP16 = 4 };
 
 /* Device error word bits (the reference's throw conditions). */
 enum {

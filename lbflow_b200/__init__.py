@@ -23,7 +23,7 @@ _lib = None
 LABEL_TYPES = {'VD': 0x1, 'GV': 0x2, 'PB': 0x4, 'VB': 0x8, 'AB': 0x10, 'BB': 0x20, 'HF': 0x40, 'SD': 0x80}
 MODELS = {'scsp': 0, 'color': 1}
 COLLISIONS = {'SRT': 0, 'MRT': 1}
-STORAGES = {'fp64': 0, 'fp16': 1, 'bf16': 2, 'fp32': 3}
+STORAGES = {'fp64': 0, 'fp16': 1, 'bf16': 2, 'fp32': 3, 'bfp16': 4}
 STEP_MACROS = 1
 STEP_ADJACENT = 2
 ERR_BITS = {1: 'Non-finite or non-positive fluid density.',

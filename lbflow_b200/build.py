@@ -49,16 +49,7 @@ def _run(cmd):
     return r
 
 
-def regenerate_moments():
-    gen = CSRC / 'gen_moments.py'
-    out = CSRC / 'moments_gen.cuh'
-    if _newer(out, [gen]):
-        text = _run([sys.executable, str(gen)]).stdout
-        out.write_text(text)
-
-
 def build(force=False, verbose=False, jobs=None):
-    regenerate_moments()
     OBJ.mkdir(exist_ok=True)
     LIB.mkdir(exist_ok=True)
     deps = _headers(CSRC) + [ROOT / 'include' / 'lbflow.h']

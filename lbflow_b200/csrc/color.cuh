@@ -17,7 +17,7 @@ struct ColorParams {
     double rho_ref[2];     // reference densities
     double relax0, relax1; // tau_k / 2 (colorfluid.cpp:241-242)
     int uniform_tau;       // tau0 == tau1: fixed MRT rates (colorfluid.cpp:317-322)
-    MrtCoef mrt;           // coefficients of the uniform rates
+    Trt rate;              // the uniform rates (used when uniform_tau)
     double ak;             // 2.25 sigma (colorfluid.cpp:305)
     double beta;           // recoloring parameter
 };
@@ -143,46 +143,30 @@ color_collide(const Grid g, const Force F, const ColorParams P, const ColorWall 
         for (int a = 0; a < 3; ++a) mo.uadj[(size_t)a * g.nfp + i] = (double)u[a];
     }
 
-    // ColorFluid::collision (colorfluid.cpp:334-387): collide the total.
+    // ColorFluid::collision (colorfluid.cpp:334-387): collide the total
+    // fT = f0 + f1 towards feq = feq_u0 + rho w (3 e.u + 4.5 (e.u)^2 - 1.5 u^2),
+    // feq_u0 = rho0 ai0 + rho1 ai1, with the same two-rate form as the
+    // single-phase step: SRT is s+ = s- = 1/tau_local; MRT uses the tau0 rates
+    // when tau0 == tau1 and getMRTS(tau_local) otherwise (simulator.cpp:199-216).
     const R usq = u[2] * u[2] + u[1] * u[1] + u[0] * u[0];
     const R uf = u[2] * Fv[2] + u[1] * Fv[1] + u[0] * Fv[0];
-    R fT[L::Q], fu0[L::Q], src[L::Q];
+    R fT[L::Q], fu0[L::Q];
 #pragma unroll
     for (int q = 0; q < L::Q; ++q) {
         fT[q] = f0[q] + f1[q];
-        const R eu = R(L::ex(q)) * u[0] + R(L::ey(q)) * u[1] + R(L::ez(q)) * u[2];
-        const R ef = R(L::ex(q)) * Fv[0] + R(L::ey(q)) * Fv[1] + R(L::ez(q)) * Fv[2];
         fu0[q] = d0 * R(P.ai[0][q]) + d1 * R(P.ai[1][q]);
-        const R feq = fu0[q] + dt * R(w<L>(q)) * (R(3) * eu + R(4.5) * eu * eu - R(1.5) * usq);
-        src[q] = R(w<L>(q)) * (R(3) * (ef - uf) + R(9) * eu * ef);
-        fT[q] = COLL == 0 ? fT[q] : feq - fT[q];   // MRT: residual
-        if (COLL == 0) {
-            fT[q] += (feq - fT[q]) / tau;
-            fT[q] += (R(1) - R(0.5) / tau) * src[q];
-        }
     }
-    if (COLL == 1) {
-        R mr[L::Q], ms[L::Q], c[L::Q];
-        mforward<R>(fT, mr);
-        mforward<R>(src, ms);
-        // fT currently holds the residual; rebuild the total before the update.
-#pragma unroll
-        for (int q = 0; q < L::Q; ++q) fT[q] = f0[q] + f1[q];
-        if (P.uniform_tau) {
-#pragma unroll
-            for (int k = 0; k < L::Q; ++k) c[k] = R(P.mrt.cr[k]) * mr[k] + R(P.mrt.cs[k]) * ms[k];
-        } else {
-            // Simulator::getMRTS at the local tau (simulator.cpp:199-216).
-            const R su = R(1) / tau;
-            const R sq = R(8) * (R(2) - su) / (R(8) - su);
-#pragma unroll
-            for (int k = 0; k < L::Q; ++k) {
-                const R s = L::rowclass(k) == kConserved ? R(0) : (L::rowclass(k) == kShear ? su : sq);
-                c[k] = (s * mr[k] + (R(1) - R(0.5) * s) * ms[k]) * R(P.mrt.inv_n[k]);
-            }
-        }
-        minverse_add<R>(c, fT);
+    R sp, sm;
+    if (COLL == 0) {
+        sp = sm = R(1) / tau;
+    } else if (P.uniform_tau) {
+        sp = R(P.rate.sp);
+        sm = R(P.rate.sm);
+    } else {
+        sp = R(1) / tau;
+        sm = R(8) * (R(2) - sp) / (R(8) - sp);
     }
+    collide_trt<L, R, true>(fT, fu0, -dt * R(1.5) * usq, dt * R(4.5), dt * R(3), u, Fv, uf, sp, sm);
 
     // ColorFluid::colorGradient (colorfluid.cpp:435-570), gradient in the
     // reference component order gr[0..D-1] = {z,y,x} / {y,x}.  The gradient

@@ -24,6 +24,7 @@ struct lbf_engine {
     std::vector<uint32_t> vox;      // voxel index of each fluid node
     size_t elem = 8;                // bytes per stored population
     void* f[2] = {nullptr, nullptr};
+    int8_t* ex[2] = {nullptr, nullptr};   // block exponents (block-scaled storage)
     int cur = 0;
     uint2* occ = nullptr;
     uint32_t* coord = nullptr;
@@ -96,32 +97,14 @@ int ecomp(int D, int q, int a)
     return kE19[q][2 - a];
 }
 
-// Simulator::getMRTS (simulator.cpp:199-216), legacy spectrum.
-void mrt_rates(int Q, double rt, double* s)
+// Two-rate form of the collision: SRT -> s+ = s- = 1/tau; MRT (legacy
+// spectrum, simulator.cpp:199-216) -> s+ = 1/tau, s- = 8 (2 - s+) / (8 - s+).
+Trt rates(bool mrt, double tau)
 {
-    const double su = 1.0 / rt;
-    const double sq = 8.0 * (2.0 - su) / (8.0 - su);
-    static const int cls9[9] = {0, 1, 1, 0, 2, 0, 2, 1, 1};
-    static const int cls19[19] = {0, 1, 1, 0, 2, 0, 2, 0, 2, 1, 1, 1, 1, 1, 1, 1, 2, 2, 2};
-    for (int k = 0; k < Q; ++k) {
-        const int c = Q == 9 ? cls9[k] : cls19[k];
-        s[k] = c == 0 ? 0.0 : (c == 1 ? su : sq);
-    }
-}
-
-template <class L>
-MrtCoef mrt_coef(double tau)
-{
-    MrtCoef m{};
-    double s[19];
-    mrt_rates(L::Q, tau, s);
-    for (int k = 0; k < L::Q; ++k) {
-        const double n = (double)rownorm2<L>(k);
-        m.cr[k] = s[k] / n;
-        m.cs[k] = (1.0 - 0.5 * s[k]) / n;
-        m.inv_n[k] = 1.0 / n;
-    }
-    return m;
+    Trt r;
+    r.sp = 1.0 / tau;
+    r.sm = mrt ? 8.0 * (2.0 - r.sp) / (8.0 - r.sp) : r.sp;
+    return r;
 }
 
 // RotateTx3D / RotateTz3D / RotateT2D (fn.cpp:118-166) and
@@ -184,7 +167,8 @@ void launch_step(lbf_engine* e, bool pull, int out)
     const void* fin = e->f[e->cur];
     void* fout = e->f[e->cur ^ 1];
     if (e->cfg.model == LBF_MODEL_SCSP) {
-        ScspLaunch a{grid_of(e), e->force, e->sp, fin, fout, macros_of(e), e->err, e->stream};
+        ScspLaunch a{grid_of(e), e->force, e->sp, fin, fout, macros_of(e), e->err, e->stream,
+                     e->ex[e->cur], e->ex[e->cur ^ 1]};
         launch_scsp(e->D, (int)e->cfg.storage, e->cfg.collision == LBF_MRT, pull, out, a);
     } else {
         ColorWall W{e->angle_id, e->angles, e->tib};
@@ -239,9 +223,58 @@ __global__ void compress_kernel(const double* __restrict__ in, typename S::T* __
         }
 }
 
+// Block-scaled storage <-> FP64 (exact decode; encode as StoreBFP16::store_blk
+// but from FP64 deviations).
+template <class L>
+__global__ void expand_blk_kernel(const int16_t* __restrict__ in, const int8_t* __restrict__ ex,
+                                  double* __restrict__ out, uint32_t nf, uint32_t nfp, double rho0)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nf) return;
+    const int e = ex[i];
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) {
+        const double w = L::w36f(q) / 36.0;
+        out[(size_t)q * nfp + i] = w * rho0 + w * ldexp((double)in[(size_t)q * nfp + i], e - 15);
+    }
+}
+
+template <class L>
+__global__ void compress_blk_kernel(const double* __restrict__ in, int16_t* __restrict__ out,
+                                    int8_t* __restrict__ ex, uint32_t nf, uint32_t nfp, double rho0)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nf) return;
+    double x[L::Q];
+    double m = 0.0;
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) {
+        const double w = L::w36f(q) / 36.0;
+        x[q] = (in[(size_t)q * nfp + i] - w * rho0) / w;
+        m = fmax(m, fabs(x[q]));
+    }
+    const int e = StoreBFP16<L>::exponent((float)m * 1.0000001f);
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) {
+        double v = rint(ldexp(x[q], 15 - e));
+        v = v > 32767.0 ? 32767.0 : (v < -32767.0 ? -32767.0 : v);
+        out[(size_t)q * nfp + i] = (int16_t)v;
+    }
+    ex[i] = (int8_t)e;
+}
+
 template <class L>
 void convert(const lbf_engine* e, bool expand, void* f, double* tmp)
 {
+    if (e->cfg.storage == LBF_STORE_BFP16) {
+        const unsigned t = 256, b = blocks_for(e->nf, t);
+        if (!b) return;
+        if (expand)
+            expand_blk_kernel<L><<<b, t, 0, e->stream>>>((const int16_t*)f, e->ex[e->cur], tmp, e->nf, e->nfp, e->cfg.rho[0]);
+        else
+            compress_blk_kernel<L><<<b, t, 0, e->stream>>>(tmp, (int16_t*)f, e->ex[e->cur], e->nf, e->nfp, e->cfg.rho[0]);
+        return;
+    }
     const unsigned t = 256, b = blocks_for(e->nf, t);
     if (!b) return;
     const double r0 = e->cfg.rho[0];
@@ -325,8 +358,9 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
         return fail(nullptr, LBF_EINVAL, "unknown fluid model");
     if (c.collision != LBF_SRT && c.collision != LBF_MRT)
         return fail(nullptr, LBF_EINVAL, "unknown collision model");
-    if (c.storage > LBF_STORE_FP32) return fail(nullptr, LBF_EINVAL, "unknown storage");
-    if (c.model == LBF_MODEL_COLOR && (c.storage == LBF_STORE_FP16 || c.storage == LBF_STORE_BF16))
+    if (c.storage > LBF_STORE_BFP16) return fail(nullptr, LBF_EINVAL, "unknown storage");
+    if (c.model == LBF_MODEL_COLOR && (c.storage == LBF_STORE_FP16 || c.storage == LBF_STORE_BF16 ||
+                                       c.storage == LBF_STORE_BFP16))
         return fail(nullptr, LBF_EINVAL, "two-phase storage must be FP64 or FP32");
     const int phases = c.model == LBF_MODEL_COLOR ? 2 : 1;
     for (int k = 0; k < phases; ++k)
@@ -344,6 +378,7 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
     e->W = (e->nx + 31) / 32;
     e->N = (size_t)c.nx * c.ny * c.nz;
     e->elem = c.storage == LBF_STORE_FP64 ? 8 : (c.storage == LBF_STORE_FP32 ? 4 : 2);
+    const bool blocked = c.storage == LBF_STORE_BFP16;
     auto bail = [&](int code, const std::string& m) { lbf_destroy(e); return fail(nullptr, code, m); };
 
     // Label checks (ValidateSimulation subset, fileprm.cpp:274-294) and the
@@ -377,7 +412,9 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
             occ[r * e->W + w] = make_uint2(bits, (uint32_t)count);
             count += (uint64_t)__builtin_popcount(bits);
         }
-    if (count >= 0xffffffffull) return bail(LBF_EINVAL, "too many fluid nodes");
+    // Element offsets inside a population buffer are 32-bit in the kernels.
+    if ((count + 64) * (uint64_t)phases * (uint64_t)e->Q >= 0xffffffffull)
+        return bail(LBF_EINVAL, "too many fluid nodes for one engine (phases * Q * nodes must stay below 2^32)");
     e->nf = (uint32_t)count;
     e->nfp = (uint32_t)((count + 63) / 64 * 64);
     if (e->nfp == 0) e->nfp = 64;
@@ -441,6 +478,10 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
         LBF_ALLOC(p, fcount * e->elem);
         e->f[b] = p;
         LBF_CUDA(cudaMemsetAsync(p, 0, fcount * e->elem, e->stream));
+        if (blocked) {
+            LBF_ALLOC(e->ex[b], e->nfp);
+            LBF_CUDA(cudaMemsetAsync(e->ex[b], 0, e->nfp, e->stream));
+        }
     }
     LBF_ALLOC(e->occ, occ.size());
     LBF_ALLOC(e->coord, e->nfp);
@@ -474,8 +515,7 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
     if (c.model == LBF_MODEL_SCSP) {
         e->sp.rho0 = c.rho[0];
         e->sp.inv_rho0 = 1.0 / c.rho[0];
-        e->sp.omega = 1.0 / c.tau[0];
-        e->sp.mrt = e->D == 3 ? mrt_coef<D3Q19>(c.tau[0]) : mrt_coef<D2Q9>(c.tau[0]);
+        e->sp.rate = rates(c.collision == LBF_MRT, c.tau[0]);
     } else {
         // ColorFluid::initPhi (colorfluid.cpp:1131-1150).
         double alpha[2];
@@ -494,7 +534,7 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
         e->cp.relax0 = c.tau[0] / 2.0;
         e->cp.relax1 = c.tau[1] / 2.0;
         e->cp.uniform_tau = c.tau[0] == c.tau[1];
-        e->cp.mrt = e->D == 3 ? mrt_coef<D3Q19>(c.tau[0]) : mrt_coef<D2Q9>(c.tau[0]);
+        e->cp.rate = rates(true, c.tau[0]);
         e->cp.ak = 2.25 * c.sigma;
         e->cp.beta = c.beta;
 
@@ -579,7 +619,7 @@ void lbf_destroy(lbf_engine* e)
     if (!e) return;
     cudaSetDevice(e->cfg.device);
     if (e->stream) cudaStreamSynchronize(e->stream);
-    void* ptrs[] = {e->f[0], e->f[1], e->occ, e->coord, e->node_label, e->node_phase, e->label_force,
+    void* ptrs[] = {e->f[0], e->f[1], e->ex[0], e->ex[1], e->occ, e->coord, e->node_label, e->node_phase, e->label_force,
                     e->rho0, e->rho1, e->u, e->uprev, e->uadj, e->ind, e->indprev, e->indadj,
                     e->phi, e->angle_id, e->angles, e->tib, e->err, e->partial, e->red};
     for (void* p : ptrs) if (p) cudaFree(p);
@@ -595,7 +635,8 @@ int lbf_initialize(lbf_engine* e)
     if (rc) return rc;
     const Grid g = grid_of(e);
     if (e->cfg.model == LBF_MODEL_SCSP)
-        launch_scsp_init(e->D, (int)e->cfg.storage, g, e->force, e->cfg.rho[0], e->f[e->cur], e->stream);
+        launch_scsp_init(e->D, (int)e->cfg.storage, g, e->force, e->cfg.rho[0], e->f[e->cur], e->ex[e->cur],
+                         e->stream);
     else
         launch_color_init(e->D, (int)e->cfg.storage, g, e->force, e->cp, e->node_phase, e->f[e->cur], e->stream);
     launch_step(e, false, kOutMacros | kOutAdjacent);

@@ -121,9 +121,9 @@ Simulation::Simulation(const Params& p) : p_(p)
     // Optional extension key (ignored by the reference's parser): population storage.
     const std::string storage = p.selector("populationStorage", "fp64", "populationStorage");
     c.storage = storage == "fp16" ? LBF_STORE_FP16 : storage == "bf16" ? LBF_STORE_BF16
-              : storage == "fp32" ? LBF_STORE_FP32 : LBF_STORE_FP64;
-    if (storage != "fp64" && storage != "fp32" && storage != "fp16" && storage != "bf16")
-        throw std::invalid_argument("populationStorage must be fp64, fp32, fp16 or bf16.");
+              : storage == "fp32" ? LBF_STORE_FP32 : storage == "bfp16" ? LBF_STORE_BFP16 : LBF_STORE_FP64;
+    if (storage != "fp64" && storage != "fp32" && storage != "fp16" && storage != "bf16" && storage != "bfp16")
+        throw std::invalid_argument("populationStorage must be fp64, fp32, fp16, bf16 or bfp16.");
     const char* dev = std::getenv("LBFLOW_DEVICE");
     c.device = dev ? std::atoi(dev) : 0;
     for (std::size_t k = 0; k < 2; ++k) {

@@ -17,6 +17,8 @@ struct ScspLaunch {
     Macros mo;
     uint32_t* err;
     cudaStream_t stream;
+    const int8_t* ein;   // block exponents of fin (block-scaled storage only)
+    int8_t* eout;
 };
 
 struct ColorLaunch {
@@ -35,7 +37,7 @@ struct ColorLaunch {
 // storage: LBF_STORE_* value; dims: 2 or 3.
 void launch_scsp(int dims, int storage, bool mrt, bool pull, int out, const ScspLaunch& a);
 void launch_scsp_init(int dims, int storage, const Grid& g, const Force& F, double rho0,
-                      void* f, cudaStream_t s);
+                      void* f, int8_t* eout, cudaStream_t s);
 void launch_color(int dims, int storage, int collision, bool pull, int out, const ColorLaunch& a);
 void launch_color_init(int dims, int storage, const Grid& g, const Force& F, const ColorParams& P,
                        const uint8_t* phase, void* f, cudaStream_t s);

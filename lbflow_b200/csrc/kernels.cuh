@@ -16,7 +16,6 @@
 #include <cuda_bf16.h>
 #include <cstdint>
 #include "lattice.cuh"
-#include "moments_gen.cuh"
 
 namespace lbf {
 
@@ -74,6 +73,7 @@ __device__ __forceinline__ uint32_t lookup(const Grid& g, int x, int y, int z, b
 // ---- storage policies -------------------------------------------------------
 // Full FP64 populations (the plain path; arithmetic close to the reference).
 struct StoreF64 {
+    static constexpr bool blocked = false;
     using T = double;
     using R = double;
     static constexpr bool shifted = false;
@@ -87,6 +87,7 @@ template <class L> struct ShiftScale {
     __device__ static float inv(int q) { return (float)L::w36f(q) / (36.0f * 4096.0f); }
 };
 template <class L> struct StoreF16 {
+    static constexpr bool blocked = false;
     using T = __half;
     using R = float;
     static constexpr bool shifted = true;
@@ -94,6 +95,7 @@ template <class L> struct StoreF16 {
     __device__ static void store(T* p, R v, int q, R) { *p = __float2half_rn(v * ShiftScale<L>::scale(q)); }
 };
 template <class L> struct StoreBF16 {
+    static constexpr bool blocked = false;
     using T = __nv_bfloat16;
     using R = float;
     static constexpr bool shifted = true;
@@ -101,6 +103,7 @@ template <class L> struct StoreBF16 {
     __device__ static void store(T* p, R v, int q, R) { *p = __float2bfloat16_rn(v * ShiftScale<L>::scale(q)); }
 };
 template <class L> struct StoreF32 {
+    static constexpr bool blocked = false;
     using T = float;
     using R = float;
     static constexpr bool shifted = true;
@@ -110,6 +113,7 @@ template <class L> struct StoreF32 {
 
 // Full (unshifted) populations in FP32 with FP32 arithmetic.
 struct StoreF32Full {
+    static constexpr bool blocked = false;
     using T = float;
     using R = float;
     static constexpr bool shifted = false;
@@ -117,54 +121,191 @@ struct StoreF32Full {
     __device__ static void store(T* p, R v, int, R) { *p = v; }
 };
 
+// Block-scaled 16-bit deviations: per node, x_q = (f_q - w_q rho0) / w_q is
+// stored as the int16 mantissa s_q = round(x_q * 2^(15 - E)), with one
+// exponent E per node chosen so that max_q |x_q| < 2^E.  The values that
+// carry a node's velocity keep 15 bits relative to the node's largest
+// deviation (IEEE FP16 keeps 11 relative to each value), for one extra byte
+// per node.  Arithmetic in FP32.
+__device__ __forceinline__ float pow2f(int e) { return __int_as_float((e + 127) << 23); }
+template <class L> struct StoreBFP16 {
+    using T = int16_t;
+    using R = float;
+    static constexpr bool shifted = true;
+    static constexpr bool blocked = true;
+    static constexpr int kEmin = -100, kEmax = 100;
+    __device__ static R load(const T*, int, R) { return R(0); }
+    __device__ static void store(T*, R, int, R) {}
+    __device__ static R load_blk(const T* p, int q, int e)
+    { return (float)__ldg(p) * (pow2f(e - 15) * ((float)L::w36f(q) / 36.0f)); }
+    // Exponent of a node whose largest |x_q| is m.
+    __device__ static int exponent(float m)
+    {
+        if (!(m > 0.0f)) return kEmin;
+        int e = ((__float_as_int(m) >> 23) & 0xff) - 126;
+        return e < kEmin ? kEmin : (e > kEmax ? kEmax : e);
+    }
+    template <int Q>
+    __device__ static void store_blk(T* base, size_t nfp, uint32_t i, const R (&g)[Q], int8_t* eout)
+    {
+        float x[Q];
+        float m = 0.0f;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            x[q] = g[q] * (36.0f / (float)L::w36f(q));
+            m = fmaxf(m, fabsf(x[q]));
+        }
+        const int e = exponent(m);
+        const float sc = pow2f(15 - e);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            int v = __float2int_rn(x[q] * sc);
+            v = v > 32767 ? 32767 : (v < -32767 ? -32767 : v);
+            base[(uint32_t)q * (uint32_t)nfp + i] = (T)v;
+        }
+        eout[i] = (int8_t)e;
+    }
+};
+
 // ---- gather: pull-stream with halfway bounce-back ----------------------------
 // src[q] receives f_q(x - e_q) after streaming, or f*_{op q}(x) when the
 // upstream voxel is solid.  nbr[q] (q >= 1) records the compact index of the
 // voxel x + e_q (the pull source of op q) or UINT32_MAX when it is solid.
+template <class S>
+__device__ __forceinline__ typename S::R load_pop(const typename S::T* p, int q, typename S::R rho0,
+                                                  const int8_t* __restrict__ ein, uint32_t src)
+{
+    if constexpr (S::blocked) return S::load_blk(p, q, (int)__ldg(&ein[src]));
+    else return S::load(p, q, rho0);
+}
+
+// Pull sources of every direction: src[q] = compact index of voxel x - e_q
+// and bit q of the returned mask set when that voxel is fluid.  The sources
+// lie in (at most) nine x-rows (y - ey, z - ez); each row's occupancy word
+// around x is loaded once and x - 1, x, x + 1 are read from it, falling back
+// to a separate lookup only at a word boundary or the periodic wrap in x.
+template <class L>
+__device__ __forceinline__ uint32_t pull_sources(const Grid& g, int x, int y, int z, uint32_t (&src)[L::Q])
+{
+    const int b = x & 31;
+    const int wx = x >> 5;
+    const uint32_t below = (1u << b) - 1u;
+    uint32_t mask = 0;
+    uint32_t rbase[9], ridx[9], rbits[9];
+    bool rload[9] = {false, false, false, false, false, false, false, false, false};
+#pragma unroll
+    for (int q = 1; q < L::Q; ++q) rload[(1 - L::ey(q)) * 3 + (1 - L::ez(q))] = true;
+#pragma unroll
+    for (int r = 0; r < 9; ++r) {
+        if (!rload[r]) continue;
+        const int dy = r / 3 - 1, dz = r % 3 - 1;
+        const int yy = dy == 0 ? y : wrap(y + dy, g.ny);
+        const int zz = (L::D == 2 || dz == 0) ? z : wrap(z + dz, g.nz);
+        rbase[r] = ((uint32_t)zz * (uint32_t)g.ny + (uint32_t)yy) * (uint32_t)g.W;
+        const uint2 e = __ldg(&g.occ[rbase[r] + wx]);
+        rbits[r] = e.x;
+        ridx[r] = e.y + __popc(e.x & below);
+    }
+#pragma unroll
+    for (int q = 1; q < L::Q; ++q) {
+        const int r = (1 - L::ey(q)) * 3 + (1 - L::ez(q));
+        const int dx = -L::ex(q);
+        const uint32_t bits = rbits[r];
+        uint32_t idx, fl;
+        if (dx == 0) {
+            fl = (bits >> b) & 1u;
+            idx = ridx[r];
+        } else if (dx < 0 && b > 0) {
+            fl = (bits >> (b - 1)) & 1u;
+            idx = ridx[r] - fl;
+        } else if (dx > 0 && b < 31 && x + 1 < g.nx) {
+            fl = (bits >> (b + 1)) & 1u;
+            idx = ridx[r] + ((bits >> b) & 1u);
+        } else {
+            const int sx = wrap(x + dx, g.nx);
+            const uint2 e = __ldg(&g.occ[rbase[r] + (sx >> 5)]);
+            const uint32_t sb = sx & 31;
+            fl = (e.x >> sb) & 1u;
+            idx = e.y + __popc(e.x & ((1u << sb) - 1u));
+        }
+        src[q] = idx;
+        mask |= fl << q;
+    }
+    return mask;
+}
+
 template <class L, class S, bool PULL>
 __device__ __forceinline__ void gather(const Grid& g, const typename S::T* __restrict__ fin,
                                        uint32_t i, int x, int y, int z,
                                        typename S::R (&f)[L::Q], uint32_t (&nbr)[L::Q],
-                                       typename S::R rho0)
+                                       typename S::R rho0, const int8_t* __restrict__ ein = nullptr)
 {
-    f[0] = S::load(fin + i, 0, rho0);
+    // Element offsets stay 32-bit (phases * Q * nfp < 2^32 is checked at
+    // creation); only the final address is 64-bit.
+    const uint32_t nfp = g.nfp;
+    f[0] = load_pop<S>(fin + i, 0, rho0, ein, i);
     nbr[0] = i;
+    if (!PULL) {
+#pragma unroll
+        for (int q = 1; q < L::Q; ++q) { f[q] = load_pop<S>(fin + (q * nfp + i), q, rho0, ein, i); nbr[q] = 0; }
+        return;
+    }
+    uint32_t src[L::Q];
+    const uint32_t mask = pull_sources<L>(g, x, y, z, src);
 #pragma unroll
     for (int q = 1; q < L::Q; ++q) {
-        if (!PULL) { f[q] = S::load(fin + (size_t)q * g.nfp + i, q, rho0); nbr[q] = 0; continue; }
-        const int sx = wrap(x - L::ex(q), g.nx);
-        const int sy = wrap(y - L::ey(q), g.ny);
-        const int sz = L::D == 3 ? wrap(z - L::ez(q), g.nz) : 0;
-        bool fluid;
-        const uint32_t j = lookup(g, sx, sy, sz, fluid);
-        nbr[L::op(q)] = fluid ? j : 0xffffffffu;
-        const typename S::T* p = fluid ? fin + (size_t)q * g.nfp + j
-                                       : fin + (size_t)L::op(q) * g.nfp + i;
-        f[q] = S::load(p, q, rho0);
+        const bool fluid = (mask >> q) & 1u;
+        const uint32_t node = fluid ? src[q] : i;
+        nbr[L::op(q)] = fluid ? src[q] : 0xffffffffu;
+        const uint32_t off = (fluid ? (uint32_t)q : (uint32_t)L::op(q)) * nfp + node;
+        f[q] = load_pop<S>(fin + off, q, rho0, ein, node);
     }
 }
 
-// ---- moments (straight-line code generated by gen_moments.py) ---------------
-template <class R> __device__ __forceinline__ void mforward(const R (&f)[9], R (&m)[9]) { forward_d2q9(f, m); }
-template <class R> __device__ __forceinline__ void mforward(const R (&f)[19], R (&m)[19]) { forward_d3q19(f, m); }
-template <class R> __device__ __forceinline__ void minverse_add(const R (&c)[9], R (&f)[9]) { inverse_add_d2q9(c, f); }
-template <class R> __device__ __forceinline__ void minverse_add(const R (&c)[19], R (&f)[19]) { inverse_add_d3q19(c, f); }
-template <class L, class R>
-__device__ __forceinline__ R mequil(int k, R rho, R rho0, const R (&u)[3], const R (&uu)[6])
-{
-    if constexpr (L::Q == 9) return meq_d2q9<R>(k, rho, rho0, u, uu);
-    else return meq_d3q19<R>(k, rho, rho0, u, uu);
-}
-template <class L, class R>
-__device__ __forceinline__ R msource(int k, const R (&F)[3], const R (&uF)[3][3], R uf)
-{
-    if constexpr (L::Q == 9) return msrc_d2q9<R>(k, F, uF, uf);
-    else return msrc_d3q19<R>(k, F, uF, uf);
-}
+// ---- collision: the reference's MRT as a two-relaxation-time update ---------
+// In the legacy D2Q9/D3Q19 spectrum (simulator.cpp:209-214) every
+// non-conserved even moment relaxes at s+ = 1/tau and every non-conserved odd
+// moment at s- = 8(2 - s+)/(8 - s+).  Because (f - feq) has zero mass moment
+// and momentum moment -F/2 (the half-force velocity shift), and the Guo term
+// is scaled by (1 - s/2), the conserved rows come out the same as with s = 0.
+// So M^-1 S M (feq - f) + M^-1 (I - S/2) M S_guo equals, per opposite pair,
+//   f_q  += -s+ (f+ - feq+) + (1 - s+/2) src+  -  s- (f- - feq-) + (1 - s-/2) src-
+//   f_q' +=   ... same even part ...           +  s- (f- - feq-) - (1 - s-/2) src-
+// with f+- = (f_q +- f_q')/2 (verified against the reference's matrices to
+// round-off in tests/test_moments.py).  SRT is the case s+ = s-.
+struct Trt { double sp, sm; };
 
-// Per-row MRT coefficients: cr[k] = s_k / |M_k|^2, cs[k] = (1 - s_k/2) / |M_k|^2,
-// inv_n[k] = 1 / |M_k|^2.
-struct MrtCoef { double cr[19], cs[19], inv_n[19]; };
+// One fused pass over the opposite pairs.  The equilibrium is written as
+//   feq_q = A_q + w_q (B + C (e.u)^2) + w_q K (e.u)
+// (single phase: A = 0, B = rho - 1.5 rho0 u^2, C = 4.5 rho0, K = 3 rho0;
+//  color: A = feq_u0, B = -1.5 rho u^2, C = 4.5 rho, K = 3 rho) and the Guo
+// source as w_q (3 (e.F - u.F) + 9 (e.u)(e.F)).
+template <class L, class R, bool HAS_A>
+__device__ __forceinline__ void collide_trt(R (&f)[L::Q], const R* A, R B, R C, R K,
+                                            const R (&u)[3], const R (&F)[3], R uf, R sp, R sm)
+{
+    const R hp = R(1) - R(0.5) * sp, hm = R(1) - R(0.5) * sm;
+    {
+        const R w0 = R(w<L>(0));
+        const R feq0 = (HAS_A ? A[0] : R(0)) + w0 * B;
+        f[0] += -sp * (f[0] - feq0) + hp * (w0 * (R(-3) * uf));
+    }
+#pragma unroll
+    for (int p = 0; p < L::NPAIR; ++p) {
+        const int q = L::pair(p), o = L::op(q);
+        const R eu = R(L::ex(q)) * u[0] + R(L::ey(q)) * u[1] + R(L::ez(q)) * u[2];
+        const R ef = R(L::ex(q)) * F[0] + R(L::ey(q)) * F[1] + R(L::ez(q)) * F[2];
+        const R wq = R(w<L>(q));
+        const R feqp = (HAS_A ? A[q] : R(0)) + wq * (B + C * eu * eu);
+        const R feqm = wq * K * eu;
+        const R fp = R(0.5) * (f[q] + f[o]);
+        const R fm = R(0.5) * (f[q] - f[o]);
+        const R ev = -sp * (fp - feqp) + hp * (wq * (R(9) * eu * ef - R(3) * uf));
+        const R od = -sm * (fm - feqm) + hm * (wq * R(3) * ef);
+        f[q] += ev + od;
+        f[o] += ev - od;
+    }
+}
 
 // ---- single-phase step (SCSP) ----------------------------------------------------
 // One launch = Simulator::streaming + bounceBack (simulator.cpp:73-111),
@@ -174,15 +315,15 @@ struct MrtCoef { double cr[19], cs[19], inv_n[19]; };
 struct ScspParams {
     double rho0;       // reference density (incompressible form, lbcfg.h:13)
     double inv_rho0;
-    double omega;      // SRT relaxation frequency 1/tau
-    MrtCoef mrt;
+    Trt rate;          // SRT: s+ = s- = 1/tau; MRT: legacy spectrum
 };
 
-template <class L, bool MRT, class S, bool PULL>
+template <class L, class S, bool PULL>
 __global__ void __launch_bounds__(128)
 scsp_step(const Grid g, const Force F, const ScspParams P,
           const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
-          Macros mo, const int out, uint32_t* __restrict__ err)
+          Macros mo, const int out, uint32_t* __restrict__ err,
+          const int8_t* __restrict__ ein, int8_t* __restrict__ eout)
 {
     using R = typename S::R;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -192,7 +333,7 @@ scsp_step(const Grid g, const Force F, const ScspParams P,
     const R rho0 = R(P.rho0);
     R f[L::Q];
     uint32_t nbr[L::Q];
-    gather<L, S, PULL>(g, fin, i, x, y, z, f, nbr, rho0);
+    gather<L, S, PULL>(g, fin, i, x, y, z, f, nbr, rho0, ein);
 
     R Fv[3];
     if (F.uniform) { Fv[0] = R(F.fx); Fv[1] = R(F.fy); Fv[2] = R(F.fz); }
@@ -201,25 +342,18 @@ scsp_step(const Grid g, const Force F, const ScspParams P,
         Fv[0] = R(lf[0]); Fv[1] = R(lf[1]); Fv[2] = R(lf[2]);
     }
 
-    R m[L::Q];
-    R rho, j[3];
-    if (MRT) {
-        mforward<R>(f, m);
-        rho = m[0];
-        j[0] = m[L::jrow(0)]; j[1] = m[L::jrow(1)]; j[2] = L::D == 3 ? m[L::jrow(2)] : R(0);
-    } else {
-        rho = f[0];
+    // SCSP::calcMacroVar + bodyForce: rho = sum f, u = sum e f / rho0 + F/(2 rho0).
+    R rho = f[0];
 #pragma unroll
-        for (int q = 1; q < L::Q; ++q) rho += f[q];
-        j[0] = j[1] = j[2] = R(0);
+    for (int q = 1; q < L::Q; ++q) rho += f[q];
+    R j[3] = {R(0), R(0), R(0)};
 #pragma unroll
-        for (int p = 0; p < L::NPAIR; ++p) {
-            const int q = L::pair(p);
-            const R b = f[q] - f[L::op(q)];
-            if (L::ex(q)) j[0] += R(L::ex(q)) * b;
-            if (L::ey(q)) j[1] += R(L::ey(q)) * b;
-            if (L::ez(q)) j[2] += R(L::ez(q)) * b;
-        }
+    for (int p = 0; p < L::NPAIR; ++p) {
+        const int q = L::pair(p);
+        const R b = f[q] - f[L::op(q)];
+        if (L::ex(q)) j[0] += R(L::ex(q)) * b;
+        if (L::ey(q)) j[1] += R(L::ey(q)) * b;
+        if (L::ez(q)) j[2] += R(L::ez(q)) * b;
     }
     const R rho_full = S::shifted ? rho0 + rho : rho;
     if (!(rho_full > R(0)) || !isfinite(rho_full)) atomicOr(err, kErrDensity);
@@ -241,50 +375,24 @@ scsp_step(const Grid g, const Force F, const ScspParams P,
         for (int a = 0; a < 3; ++a) mo.uadj[(size_t)a * g.nfp + i] = (double)u[a];
     }
 
-    if (MRT) {
-        const R uu[6] = {u[0] * u[0], u[1] * u[1], u[2] * u[2], u[0] * u[1], u[0] * u[2], u[1] * u[2]};
-        R uF[3][3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int b = 0; b < 3; ++b) uF[a][b] = u[a] * Fv[b];
-        R c[L::Q];
-#pragma unroll
-        for (int k = 0; k < L::Q; ++k) {
-            if (L::rowclass(k) == kConserved) {
-                // s = 0: only the force moment survives (0 for mass, F for momentum).
-                R v = R(0);
-                if (k == L::jrow(0)) v = Fv[0];
-                else if (k == L::jrow(1)) v = Fv[1];
-                else if (L::D == 3 && k == L::jrow(2)) v = Fv[2];
-                c[k] = v * R(P.mrt.inv_n[k]);
-            } else {
-                c[k] = R(P.mrt.cr[k]) * (mequil<L, R>(k, rho, rho0, u, uu) - m[k])
-                     + R(P.mrt.cs[k]) * msource<L, R>(k, Fv, uF, uf);
-            }
-        }
-        minverse_add<R>(c, f);
+    // Equilibrium w (rho + rho0 (3 e.u + 4.5 (e.u)^2 - 1.5 u^2)) (scsp.cpp:398-402)
+    // and Guo source (simulator.cpp:230-246), relaxed in the two-rate form.
+    collide_trt<L, R, false>(f, nullptr, rho - rho0 * R(1.5) * usq, rho0 * R(4.5), rho0 * R(3),
+                             u, Fv, uf, R(P.rate.sp), R(P.rate.sm));
+
+    if constexpr (S::blocked) {
+        S::store_blk(fout, g.nfp, i, f, eout);
     } else {
-        const R om = R(P.omega);
-        const R fo = R(1) - R(0.5) * om;
 #pragma unroll
-        for (int q = 0; q < L::Q; ++q) {
-            const R eu = R(L::ex(q)) * u[0] + R(L::ey(q)) * u[1] + R(L::ez(q)) * u[2];
-            const R ef = R(L::ex(q)) * Fv[0] + R(L::ey(q)) * Fv[1] + R(L::ez(q)) * Fv[2];
-            const R wq = R(w<L>(q));
-            const R feq = wq * (rho + rho0 * (R(3) * eu + R(4.5) * eu * eu - R(1.5) * usq));
-            const R src = wq * (R(3) * (ef - uf) + R(9) * eu * ef);
-            f[q] += (feq - f[q]) * om + fo * src;
-        }
+        for (int q = 0; q < L::Q; ++q) S::store(fout + (q * g.nfp + i), f[q], q, rho0);
     }
-#pragma unroll
-    for (int q = 0; q < L::Q; ++q) S::store(fout + (size_t)q * g.nfp + i, f[q], q, rho0);
 }
 
 // t = 0 populations of SCSP::initialize (scsp.cpp:116-134):
 // f_q = w_q rho0 - 1.5 w_q (e_q . F).
 template <class L, class S>
-__global__ void scsp_init(const Grid g, const Force F, double rho0, typename S::T* __restrict__ f)
+__global__ void scsp_init(const Grid g, const Force F, double rho0, typename S::T* __restrict__ f,
+                          int8_t* __restrict__ eout)
 {
     using R = typename S::R;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -292,6 +400,7 @@ __global__ void scsp_init(const Grid g, const Force F, double rho0, typename S::
     double Fv[3];
     if (F.uniform) { Fv[0] = F.fx; Fv[1] = F.fy; Fv[2] = F.fz; }
     else { const double* lf = F.label_force + 3 * F.label[i]; Fv[0] = lf[0]; Fv[1] = lf[1]; Fv[2] = lf[2]; }
+    R vals[L::Q];
 #pragma unroll
     for (int q = 0; q < L::Q; ++q) {
         const double wq = L::w36f(q) / 36.0;
@@ -302,7 +411,13 @@ __global__ void scsp_init(const Grid g, const Force F, double rho0, typename S::
         ef += L::ex(q) * Fv[0];
         double v = wq * rho0;
         v -= 1.5 * wq * ef;
-        S::store(f + (size_t)q * g.nfp + i, S::shifted ? R(v - wq * rho0) : R(v), q, R(rho0));
+        vals[q] = S::shifted ? R(v - wq * rho0) : R(v);
+    }
+    if constexpr (S::blocked) {
+        S::store_blk(f, g.nfp, i, vals, eout);
+    } else {
+#pragma unroll
+        for (int q = 0; q < L::Q; ++q) S::store(f + (size_t)q * g.nfp + i, vals[q], q, R(rho0));
     }
 }
 

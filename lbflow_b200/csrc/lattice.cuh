@@ -5,16 +5,14 @@
 // of the population checkpoint.  Components are stored here as (x, y, z),
 // whereas the reference stores them {y,x} / {z,y,x}; the values are the same.
 //
-// Besides the vectors, each descriptor carries the MRT transform M
-// (solver/src/lbm/simulator.cpp:162-197) as integers and the relaxation class
-// of every moment row (simulator.cpp:209-214).  The moment-space arithmetic
-// itself is generated straight-line code (gen_moments.py -> moments_gen.cuh).
+// The reference's MRT transform (solver/src/lbm/simulator.cpp:162-197) is not
+// needed on the device: with its legacy rates the collision is a two-rate
+// update of opposite-direction pairs (kernels.cuh, collide_trt), so the
+// descriptor carries the pairing instead.
 #pragma once
 #include <cstdint>
 
 namespace lbf {
-
-enum RowClass : int { kConserved = 0, kShear = 1, kKinetic = 2 };
 
 struct D2Q9 {
     static constexpr int D = 2, Q = 9, NPAIR = 4;
@@ -32,22 +30,6 @@ struct D2Q9 {
     // One representative of each opposite pair.
     __host__ __device__ static constexpr int pair(int i)
     { constexpr int t[4] = {1, 2, 5, 6}; return t[i]; }
-    __host__ __device__ static constexpr int M(int i, int j)
-    { constexpr int t[9][9] = {
-        { 1, 1, 1, 1, 1, 1, 1, 1, 1},
-        {-4,-1,-1,-1,-1, 2, 2, 2, 2},
-        { 4,-2,-2,-2,-2, 1, 1, 1, 1},
-        { 0, 1, 0,-1, 0, 1,-1,-1, 1},
-        { 0,-2, 0, 2, 0, 1,-1,-1, 1},
-        { 0, 0, 1, 0,-1, 1, 1,-1,-1},
-        { 0, 0,-2, 0, 2, 1, 1,-1,-1},
-        { 0, 1,-1, 1,-1, 0, 0, 0, 0},
-        { 0, 0, 0, 0, 0, 1,-1, 1,-1}}; return t[i][j]; }
-    __host__ __device__ static constexpr int rowclass(int i)
-    { constexpr int t[9] = {0, 1, 1, 0, 2, 0, 2, 1, 1}; return t[i]; }
-    // Rows of M that are the momentum (jx, jy, jz); jz absent in 2D.
-    __host__ __device__ static constexpr int jrow(int i)
-    { constexpr int t[3] = {3, 5, -1}; return t[i]; }
     // Color-gradient and perturbation weights (colorfluid.cpp:1152-1168).
     __host__ __device__ static constexpr double B(int i)
     { constexpr double t[9] = {-4.0/27, 2.0/27, 2.0/27, 2.0/27, 2.0/27,
@@ -73,31 +55,6 @@ struct D3Q19 {
     __host__ __device__ static constexpr int w36f(int q) { return q == 0 ? 12 : (q < 7 ? 2 : 1); }
     __host__ __device__ static constexpr int pair(int i)
     { constexpr int t[9] = {1, 3, 5, 7, 8, 11, 12, 15, 16}; return t[i]; }
-    __host__ __device__ static constexpr int M(int i, int j)
-    { constexpr int t[19][19] = {
-        {  1,  1,  1,  1,  1,  1,  1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1},
-        {-30,-11,-11,-11,-11,-11,-11, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8, 8},
-        { 12, -4, -4, -4, -4, -4, -4, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1},
-        {  0,  1, -1,  0,  0,  0,  0, 1,-1, 1,-1, 1,-1, 1,-1, 0, 0, 0, 0},
-        {  0, -4,  4,  0,  0,  0,  0, 1,-1, 1,-1, 1,-1, 1,-1, 0, 0, 0, 0},
-        {  0,  0,  0,  1, -1,  0,  0, 1, 1,-1,-1, 0, 0, 0, 0, 1,-1, 1,-1},
-        {  0,  0,  0, -4,  4,  0,  0, 1, 1,-1,-1, 0, 0, 0, 0, 1,-1, 1,-1},
-        {  0,  0,  0,  0,  0,  1, -1, 0, 0, 0, 0, 1, 1,-1,-1, 1, 1,-1,-1},
-        {  0,  0,  0,  0,  0, -4,  4, 0, 0, 0, 0, 1, 1,-1,-1, 1, 1,-1,-1},
-        {  0,  2,  2, -1, -1, -1, -1, 1, 1, 1, 1, 1, 1, 1, 1,-2,-2,-2,-2},
-        {  0, -4, -4,  2,  2,  2,  2, 1, 1, 1, 1, 1, 1, 1, 1,-2,-2,-2,-2},
-        {  0,  0,  0,  1,  1, -1, -1, 1, 1, 1, 1,-1,-1,-1,-1, 0, 0, 0, 0},
-        {  0,  0,  0, -2, -2,  2,  2, 1, 1, 1, 1,-1,-1,-1,-1, 0, 0, 0, 0},
-        {  0,  0,  0,  0,  0,  0,  0, 1,-1,-1, 1, 0, 0, 0, 0, 0, 0, 0, 0},
-        {  0,  0,  0,  0,  0,  0,  0, 0, 0, 0, 0, 0, 0, 0, 0, 1,-1,-1, 1},
-        {  0,  0,  0,  0,  0,  0,  0, 0, 0, 0, 0, 1,-1,-1, 1, 0, 0, 0, 0},
-        {  0,  0,  0,  0,  0,  0,  0, 1,-1, 1,-1,-1, 1,-1, 1, 0, 0, 0, 0},
-        {  0,  0,  0,  0,  0,  0,  0,-1,-1, 1, 1, 0, 0, 0, 0, 1,-1, 1,-1},
-        {  0,  0,  0,  0,  0,  0,  0, 0, 0, 0, 0, 1, 1,-1,-1,-1,-1, 1, 1}}; return t[i][j]; }
-    __host__ __device__ static constexpr int rowclass(int i)
-    { constexpr int t[19] = {0, 1, 1, 0, 2, 0, 2, 0, 2, 1, 1, 1, 1, 1, 1, 1, 2, 2, 2}; return t[i]; }
-    __host__ __device__ static constexpr int jrow(int i)
-    { constexpr int t[3] = {3, 5, 7}; return t[i]; }
     __host__ __device__ static constexpr double B(int i)
     { constexpr double t[19] = {
         -(2.0 + 2.0*2) / (3.0*2 + 12.0),
@@ -119,9 +76,6 @@ struct D3Q19 {
 template <class L> __host__ __device__ constexpr int comp(int q, int a)
 { return a == 0 ? L::ex(q) : (a == 1 ? L::ey(q) : L::ez(q)); }
 
-// Squared norm of row k (M^-1 = M^T diag(1/|M_k|^2) for a row-orthogonal M); host use.
-template <class L> constexpr int rownorm2(int k)
-{ int s = 0; for (int q = 0; q < L::Q; ++q) s += L::M(k, q) * L::M(k, q); return s; }
 template <class L> __host__ __device__ constexpr double w(int q) { return L::w36f(q) / 36.0; }
 template <class L> __host__ __device__ constexpr bool axis_dir(int q)
 { return (L::ex(q) != 0) + (L::ey(q) != 0) + (L::ez(q) != 0) == 1; }

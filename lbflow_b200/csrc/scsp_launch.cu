@@ -13,14 +13,11 @@ void dispatch(bool mrt, bool pull, int out, const ScspLaunch& a)
     T* fout = static_cast<T*>(a.fout);
     const unsigned threads = 128, blocks = blocks_for(a.g.nf, threads);
     if (blocks == 0) return;
-#define LBF_SCSP(MRT, PULL) \
-    scsp_step<L, MRT, S, PULL><<<blocks, threads, 0, a.stream>>>(a.g, a.F, a.P, fin, fout, a.mo, out, a.err)
-    if (pull) {
-        if (mrt) LBF_SCSP(true, true); else LBF_SCSP(false, true);
-    } else {
-        if (mrt) LBF_SCSP(true, false); else LBF_SCSP(false, false);
-    }
-#undef LBF_SCSP
+    (void)mrt;   // the collision rates (SRT or MRT) are in a.P.rate
+    if (pull)
+        scsp_step<L, S, true><<<blocks, threads, 0, a.stream>>>(a.g, a.F, a.P, fin, fout, a.mo, out, a.err, a.ein, a.eout);
+    else
+        scsp_step<L, S, false><<<blocks, threads, 0, a.stream>>>(a.g, a.F, a.P, fin, fout, a.mo, out, a.err, a.ein, a.eout);
 }
 
 template <class L>
@@ -30,20 +27,22 @@ void dispatch_storage(int storage, bool mrt, bool pull, int out, const ScspLaunc
     case LBF_STORE_FP64: dispatch<L, StoreF64>(mrt, pull, out, a); break;
     case LBF_STORE_FP16: dispatch<L, StoreF16<L>>(mrt, pull, out, a); break;
     case LBF_STORE_BF16: dispatch<L, StoreBF16<L>>(mrt, pull, out, a); break;
+    case LBF_STORE_BFP16: dispatch<L, StoreBFP16<L>>(mrt, pull, out, a); break;
     default: dispatch<L, StoreF32<L>>(mrt, pull, out, a); break;
     }
 }
 
 template <class L>
-void init_storage(int storage, const Grid& g, const Force& F, double rho0, void* f, cudaStream_t s)
+void init_storage(int storage, const Grid& g, const Force& F, double rho0, void* f, int8_t* e, cudaStream_t s)
 {
     const unsigned threads = 256, blocks = blocks_for(g.nf, threads);
     if (blocks == 0) return;
     switch (storage) {
-    case LBF_STORE_FP64: scsp_init<L, StoreF64><<<blocks, threads, 0, s>>>(g, F, rho0, (double*)f); break;
-    case LBF_STORE_FP16: scsp_init<L, StoreF16<L>><<<blocks, threads, 0, s>>>(g, F, rho0, (__half*)f); break;
-    case LBF_STORE_BF16: scsp_init<L, StoreBF16<L>><<<blocks, threads, 0, s>>>(g, F, rho0, (__nv_bfloat16*)f); break;
-    default: scsp_init<L, StoreF32<L>><<<blocks, threads, 0, s>>>(g, F, rho0, (float*)f); break;
+    case LBF_STORE_FP64: scsp_init<L, StoreF64><<<blocks, threads, 0, s>>>(g, F, rho0, (double*)f, e); break;
+    case LBF_STORE_FP16: scsp_init<L, StoreF16<L>><<<blocks, threads, 0, s>>>(g, F, rho0, (__half*)f, e); break;
+    case LBF_STORE_BF16: scsp_init<L, StoreBF16<L>><<<blocks, threads, 0, s>>>(g, F, rho0, (__nv_bfloat16*)f, e); break;
+    case LBF_STORE_BFP16: scsp_init<L, StoreBFP16<L>><<<blocks, threads, 0, s>>>(g, F, rho0, (int16_t*)f, e); break;
+    default: scsp_init<L, StoreF32<L>><<<blocks, threads, 0, s>>>(g, F, rho0, (float*)f, e); break;
     }
 }
 }  // namespace
@@ -55,10 +54,10 @@ void launch_scsp(int dims, int storage, bool mrt, bool pull, int out, const Scsp
 }
 
 void launch_scsp_init(int dims, int storage, const Grid& g, const Force& F, double rho0,
-                      void* f, cudaStream_t s)
+                      void* f, int8_t* e, cudaStream_t s)
 {
-    if (dims == 3) init_storage<D3Q19>(storage, g, F, rho0, f, s);
-    else init_storage<D2Q9>(storage, g, F, rho0, f, s);
+    if (dims == 3) init_storage<D3Q19>(storage, g, F, rho0, f, e, s);
+    else init_storage<D2Q9>(storage, g, F, rho0, f, e, s);
 }
 
 }  // namespace lbf

@@ -1,0 +1,78 @@
+"""Run an engine to steady state and measure the body-force permeability.
+
+converge() applies LBFlow's stopping rule (Simulator::updateConvergence,
+solver/src/lbm/simulator.cpp:248-325) with the engine's device reductions: at
+every report step the relative L2 change of the velocity field since the last
+report, sqrt(sum (u - u_prev)^2 / sum u^2), and the same against the previous
+step must be below `tol` (or their RMS below 1e-12) for three consecutive
+reports.  permeability() is scripts/rock_workflow.py:60-66 /
+porous_media.py:20-44: K = nu <u_x> / g_x with <u_x> averaged over all voxels
+and nu = (tau - 1/2) / 3.
+"""
+import math
+import time
+
+import numpy as np
+
+
+def permeability(engine, tau, g, axis=0):
+    s = engine.flux_sums()
+    mean = s[axis] / engine.N
+    return (tau - 0.5) / 3.0 * mean / g
+
+
+def converge(engine, tau, g, report=1000, tol=1e-6, max_steps=2_000_000, initialized=False,
+             on_report=None):
+    """Step to the reference's convergence criterion; returns a dict with the
+    completed steps, wall seconds (device work included), K and the residual history."""
+    if not initialized:
+        engine.initialize()
+    D = engine.dims
+    count = D * engine.N
+    t = 0
+    stable = 0
+    first = True
+    history = []
+    engine.synchronize()
+    t0 = time.perf_counter()
+    while t < max_steps:
+        engine.step(report - 1, adjacent=True)
+        engine.step(1, macros=True)
+        t += report
+        engine.check()
+        K = permeability(engine, tau, g)
+        if first:
+            engine.convergence(first=True)
+            first = False
+            history.append((t, float('nan'), float('nan'), K, time.perf_counter() - t0))
+            continue
+        s = engine.convergence()
+        if not all(math.isfinite(v) for v in s[:3]):
+            raise RuntimeError('Invalid global velocity residual.')
+        rms = math.sqrt(s[0] / count)
+        res = math.sqrt(s[0] / s[1]) if s[1] > 0 else 0.0
+        arms = math.sqrt(s[2] / count)
+        ares = math.sqrt(s[2] / s[1]) if s[1] > 0 else 0.0
+        ok = (rms <= 1e-12 or res < tol) and (arms <= 1e-12 or ares < tol)
+        stable = stable + 1 if ok else 0
+        history.append((t, res, ares, K, time.perf_counter() - t0))
+        if on_report:
+            on_report(t, res, ares)
+        if stable >= 3:
+            break
+    engine.synchronize()
+    seconds = time.perf_counter() - t0
+    return dict(steps=t, seconds=seconds, K=permeability(engine, tau, g), converged=stable >= 3,
+                history=history)
+
+
+def time_to_band(history, K_ref, rel=1e-3):
+    """First report after which K stays within rel of K_ref: (steps, seconds) or None."""
+    hit = None
+    for t, _, _, K, sec in history:
+        if abs(K - K_ref) <= rel * abs(K_ref):
+            if hit is None:
+                hit = (t, sec)
+        else:
+            hit = None
+    return hit
