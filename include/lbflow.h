@@ -172,6 +172,51 @@ int lbf_synchronize(lbf_engine *e);
  * for callers that time or order work against it. */
 void *lbf_stream(const lbf_engine *e);
 
+/* ---- Batched geometries ----------------------------------------------------
+ * Many independent single-phase D3Q19 geometries of uneven size advanced
+ * together: one launch per step walks a packed list of fluid-node tiles of all
+ * active geometries (all-solid regions produce no tiles), each tile using its
+ * geometry's size and relaxation time; plain steps are replayed from a CUDA
+ * graph; per-geometry reductions let each geometry converge and retire on its
+ * own.  No counterpart in the reference, which runs one geometry per process
+ * (scripts/benchmarks.py:221-224 farms cases out to a thread pool). */
+typedef struct {
+    uint32_t nx, ny, nz;      /* voxels */
+    const uint8_t *labels;    /* nx*ny*nz labels, x fastest (copied) */
+    double tau;               /* relaxation time of this geometry */
+} lbf_batch_geometry;
+
+typedef struct lbf_batch lbf_batch;
+
+/* labels: the shared label table; collision: LBF_SRT or LBF_MRT; storage:
+ * LBF_STORE_FP64, _FP32 or _FP16; rho0: reference density. */
+int lbf_batch_create(const lbf_batch_geometry *geoms, uint32_t count, const lbf_label labels[256],
+                     uint32_t collision, uint32_t storage, int32_t device, double rho0, lbf_batch **out);
+void lbf_batch_destroy(lbf_batch *b);
+/* t = 0 stage for every geometry (as lbf_initialize). */
+int lbf_batch_initialize(lbf_batch *b);
+/* nsteps steps of every active geometry; flags as for lbf_step. */
+int lbf_batch_step(lbf_batch *b, uint32_t nsteps, uint32_t flags);
+/* Per geometry, the lbf_convergence sums: out[count][6]. */
+int lbf_batch_convergence(lbf_batch *b, int first, double *out);
+/* Per geometry, the lbf_flux_sums: out[count][9]. */
+int lbf_batch_flux_sums(lbf_batch *b, double *out);
+/* active[count]: 0 retires a geometry from the step schedule. */
+int lbf_batch_set_active(lbf_batch *b, const uint8_t *active);
+/* Times tile size and grid shape candidates over `steps` steps each and keeps
+ * the fastest; the populations are restored afterwards.  out = { threads,
+ * tile nodes, 128-thread blocks per SM, ms per step }. */
+int lbf_batch_autotune(lbf_batch *b, uint32_t steps, double out[4]);
+/* Dense fields of one geometry from the last step that wrote macros. */
+int lbf_batch_get_macros(lbf_batch *b, uint32_t geometry, double *rho, double *u);
+int lbf_batch_status(lbf_batch *b, uint32_t *bits);
+int lbf_batch_synchronize(lbf_batch *b);
+/* Fluid nodes of one geometry, or of all with geometry = UINT32_MAX. */
+uint64_t lbf_batch_fluid_nodes(const lbf_batch *b, uint32_t geometry);
+uint32_t lbf_batch_active_tiles(const lbf_batch *b);
+void *lbf_batch_stream(const lbf_batch *b);
+const char *lbf_batch_last_error(const lbf_batch *b);
+
 /* Pore-measure sums of lbf_flux_sums over arrays the caller already holds on
  * the device, for callers that cannot allocate device memory (a frozen or
  * exhausted memory pool, an allocator that owns the whole device).  Nothing

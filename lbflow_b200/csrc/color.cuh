@@ -67,7 +67,10 @@ color_phase(const Grid g, const typename S::T* __restrict__ fin, double* __restr
     for (int q = 1; q < L::Q; ++q) { d0 += f0[q]; d1 += f1[q]; }
     const R dt = d0 + d1;
     if (!isfinite(d0) || !isfinite(d1) || !isfinite(dt) || !(dt > R(0))) atomicOr(err, kErrDensity);
-    if (d0 < R(-1e-10) * dt || d1 < R(-1e-10) * dt) atomicOr(err, kErrComponent);
+    // The reference's roundoff allowance, -1e-10 rho (colorfluid.cpp:258), is
+    // about 450 FP64 ulps; at FP32 arithmetic the same 450 ulps is 2.7e-5 rho.
+    const R tol = sizeof(R) == 8 ? R(1e-10) : R(2.7e-5);
+    if (d0 < -tol * dt || d1 < -tol * dt) atomicOr(err, kErrComponent);
     phi[i] = (double)((d0 - d1) / dt);
 }
 

@@ -318,16 +318,16 @@ struct ScspParams {
     Trt rate;          // SRT: s+ = s- = 1/tau; MRT: legacy spectrum
 };
 
+// Update of one fluid node i (the body of scsp_step, shared with the batched
+// kernel).
 template <class L, class S, bool PULL>
-__global__ void __launch_bounds__(128)
-scsp_step(const Grid g, const Force F, const ScspParams P,
-          const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
-          Macros mo, const int out, uint32_t* __restrict__ err,
-          const int8_t* __restrict__ ein, int8_t* __restrict__ eout)
+__device__ __forceinline__ void scsp_update(const Grid& g, const Force& F, const ScspParams& P,
+                                            const typename S::T* __restrict__ fin,
+                                            typename S::T* __restrict__ fout, const uint32_t i,
+                                            const Macros& mo, const int out, uint32_t* __restrict__ err,
+                                            const int8_t* __restrict__ ein, int8_t* __restrict__ eout)
 {
     using R = typename S::R;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.nf) return;
     int x, y, z;
     unpack(__ldg(&g.coord[i]), x, y, z);
     const R rho0 = R(P.rho0);
@@ -386,6 +386,18 @@ scsp_step(const Grid g, const Force F, const ScspParams P,
 #pragma unroll
         for (int q = 0; q < L::Q; ++q) S::store(fout + (q * g.nfp + i), f[q], q, rho0);
     }
+}
+
+template <class L, class S, bool PULL>
+__global__ void __launch_bounds__(128)
+scsp_step(const Grid g, const Force F, const ScspParams P,
+          const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
+          Macros mo, const int out, uint32_t* __restrict__ err,
+          const int8_t* __restrict__ ein, int8_t* __restrict__ eout)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.nf) return;
+    scsp_update<L, S, PULL>(g, F, P, fin, fout, i, mo, out, err, ein, eout);
 }
 
 // t = 0 populations of SCSP::initialize (scsp.cpp:116-134):
