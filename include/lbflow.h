@@ -113,6 +113,16 @@ void lbf_destroy(lbf_engine *e);
  * t = 0 macroscopic fields are kept for lbf_get_macros. */
 int lbf_initialize(lbf_engine *e);
 
+/* Warm start (single-phase only): as lbf_initialize, but the t = 0
+ * populations are the equilibrium of given fields instead of the fluid at
+ * rest.  fields: DEVICE memory on the engine's device, one record of `ld`
+ * floats (ld >= 4) per voxel in (z, y, x) order, x fastest: velocity x, y, z
+ * (the macroscopic velocity, half force included) and density.  Solid voxels
+ * are ignored.  The read happens on the engine's stream; the caller keeps
+ * the array alive until lbf_synchronize or any blocking call returns.
+ * flags: reserved, 0. */
+int lbf_initialize_equilibrium(lbf_engine *e, const float *fields, uint32_t ld, uint32_t flags);
+
 /* nsteps steps of the Run loop body: streaming, bounce-back, calcMacroVar,
  * bodyForce, collision (scsp.cpp:75-104; colorfluid.cpp:142-198).  flags
  * (LBF_STEP_*) apply to the last step of the call. */

@@ -77,6 +77,7 @@ def library():
             'lbf_create': (I, [ctypes.POINTER(_Config), ctypes.POINTER(_Label), ctypes.c_char_p, ctypes.POINTER(P)]),
             'lbf_destroy': (None, [P]),
             'lbf_initialize': (I, [P]),
+            'lbf_initialize_equilibrium': (I, [P, P, U32, U32]),
             'lbf_step': (I, [P, U32, U32]),
             'lbf_get_populations': (I, [P, D, ctypes.c_size_t]),
             'lbf_set_populations': (I, [P, D, ctypes.c_size_t]),
@@ -185,6 +186,11 @@ class Engine:
 
     def initialize(self):
         self._ck(self._lib.lbf_initialize(self._h))
+
+    def initialize_equilibrium(self, fields_ptr, ld=4):
+        """Warm start from device fields: `fields_ptr` is the device address of a
+        dense float32 (z, y, x, ld) array holding velocity x, y, z and density."""
+        self._ck(self._lib.lbf_initialize_equilibrium(self._h, ctypes.c_void_p(int(fields_ptr)), int(ld), 0))
 
     def step(self, n=1, macros=False, adjacent=False):
         flags = (STEP_MACROS if macros else 0) | (STEP_ADJACENT if adjacent else 0)

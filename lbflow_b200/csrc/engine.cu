@@ -645,6 +645,28 @@ int lbf_initialize(lbf_engine* e)
     return LBF_OK;
 }
 
+int lbf_initialize_equilibrium(lbf_engine* e, const float* fields, uint32_t ld, uint32_t flags)
+{
+    if (!e) return fail(e, LBF_EINVAL, "NULL engine");
+    if (!fields || ld < 4 || flags != 0) return fail(e, LBF_EINVAL, "fields must be non-NULL with ld >= 4; flags 0");
+    if (e->cfg.model != LBF_MODEL_SCSP) return fail(e, LBF_EINVAL, "equilibrium initialisation is single-phase only");
+    int rc = setdev(e);
+    if (rc) return rc;
+    cudaPointerAttributes pa{};
+    if (cudaPointerGetAttributes(&pa, fields) != cudaSuccess || pa.type != cudaMemoryTypeDevice ||
+        pa.device != e->cfg.device) {
+        cudaGetLastError();
+        return fail(e, LBF_EINVAL, "fields must be device memory of the engine's device");
+    }
+    const Grid g = grid_of(e);
+    launch_scsp_init_eq(e->D, (int)e->cfg.storage, g, e->force, e->cfg.rho[0], fields, ld, e->f[e->cur],
+                        e->ex[e->cur], e->stream);
+    launch_step(e, false, kOutMacros | kOutAdjacent);
+    LBF_CK(e, cudaGetLastError());
+    e->initialized = true;
+    return LBF_OK;
+}
+
 int lbf_step(lbf_engine* e, uint32_t nsteps, uint32_t flags)
 {
     if (!e) return fail(e, LBF_EINVAL, "NULL engine");

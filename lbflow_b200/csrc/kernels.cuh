@@ -433,4 +433,46 @@ __global__ void scsp_init(const Grid g, const Force F, double rho0, typename S::
     }
 }
 
+// Warm start: equilibrium populations of given per-voxel fields.  fields is
+// a dense (z, y, x) array of records of `ld` floats: velocity x, y, z (the
+// physical velocity, half force included) and density.  The raw momentum is
+// rho0 * (u - F / (2 rho0)), as the macroscopic velocity of SCSP::calcMacroVar
+// (solver/src/lbm/scsp.cpp:136-175) adds the half force back; the
+// populations are the incompressible equilibrium of SCSP::equilSRT
+// (scsp.cpp:374-409) at that momentum.
+template <class L, class S>
+__global__ void scsp_init_eq(const Grid g, const Force F, double rho0, const float* __restrict__ fields,
+                             uint32_t ld, typename S::T* __restrict__ f, int8_t* __restrict__ eout)
+{
+    using R = typename S::R;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.nf) return;
+    const uint32_t c = g.coord[i];
+    const size_t vox = ((size_t)(c >> 22) * g.ny + ((c >> 11) & 0x7FFu)) * g.nx + (c & 0x7FFu);
+    const float* r = fields + vox * ld;
+    double Fv[3];
+    if (F.uniform) { Fv[0] = F.fx; Fv[1] = F.fy; Fv[2] = F.fz; }
+    else { const double* lf = F.label_force + 3 * F.label[i]; Fv[0] = lf[0]; Fv[1] = lf[1]; Fv[2] = lf[2]; }
+    double v[3];
+    for (int d = 0; d < 3; ++d) v[d] = (double)r[d] - Fv[d] / (2.0 * rho0);
+    if (L::D == 2) v[2] = 0.0;
+    const double rho = (double)r[3];
+    const double vv = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    R vals[L::Q];
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) {
+        const double wq = L::w36f(q) / 36.0;
+        double ev = L::ex(q) * v[0] + L::ey(q) * v[1];
+        if (L::D == 3) ev += L::ez(q) * v[2];
+        const double fq = wq * (rho + rho0 * (3.0 * ev + 4.5 * ev * ev - 1.5 * vv));
+        vals[q] = S::shifted ? R(fq - wq * rho0) : R(fq);
+    }
+    if constexpr (S::blocked) {
+        S::store_blk(f, g.nfp, i, vals, eout);
+    } else {
+#pragma unroll
+        for (int q = 0; q < L::Q; ++q) S::store(f + (size_t)q * g.nfp + i, vals[q], q, R(rho0));
+    }
+}
+
 }  // namespace lbf

@@ -45,7 +45,28 @@ void init_storage(int storage, const Grid& g, const Force& F, double rho0, void*
     default: scsp_init<L, StoreF32<L>><<<blocks, threads, 0, s>>>(g, F, rho0, (float*)f, e); break;
     }
 }
+template <class L>
+void init_eq_storage(int storage, const Grid& g, const Force& F, double rho0, const float* fields, uint32_t ld,
+                     void* f, int8_t* e, cudaStream_t s)
+{
+    const unsigned threads = 256, blocks = blocks_for(g.nf, threads);
+    if (blocks == 0) return;
+    switch (storage) {
+    case LBF_STORE_FP64: scsp_init_eq<L, StoreF64><<<blocks, threads, 0, s>>>(g, F, rho0, fields, ld, (double*)f, e); break;
+    case LBF_STORE_FP16: scsp_init_eq<L, StoreF16<L>><<<blocks, threads, 0, s>>>(g, F, rho0, fields, ld, (__half*)f, e); break;
+    case LBF_STORE_BF16: scsp_init_eq<L, StoreBF16<L>><<<blocks, threads, 0, s>>>(g, F, rho0, fields, ld, (__nv_bfloat16*)f, e); break;
+    case LBF_STORE_BFP16: scsp_init_eq<L, StoreBFP16<L>><<<blocks, threads, 0, s>>>(g, F, rho0, fields, ld, (int16_t*)f, e); break;
+    default: scsp_init_eq<L, StoreF32<L>><<<blocks, threads, 0, s>>>(g, F, rho0, fields, ld, (float*)f, e); break;
+    }
+}
 }  // namespace
+
+void launch_scsp_init_eq(int dims, int storage, const Grid& g, const Force& F, double rho0, const float* fields,
+                         uint32_t ld, void* f, int8_t* e, cudaStream_t s)
+{
+    if (dims == 3) init_eq_storage<D3Q19>(storage, g, F, rho0, fields, ld, f, e, s);
+    else init_eq_storage<D2Q9>(storage, g, F, rho0, fields, ld, f, e, s);
+}
 
 void launch_scsp(int dims, int storage, bool mrt, bool pull, int out, const ScspLaunch& a)
 {

@@ -1,4 +1,4 @@
-"""The C-ABI library: loads, exports what include/lbflow.h declares, validates input (no GPU needed)."""
+"""The C-ABI library: loads, exports what include/*.h declare, validates input (no GPU needed)."""
 import ctypes
 import re
 from pathlib import Path
@@ -10,7 +10,7 @@ ROOT = Path(__file__).resolve().parent.parent
 
 
 def declared_functions():
-    text = (ROOT / 'include' / 'lbflow.h').read_text()
+    text = ''.join(p.read_text() for p in sorted((ROOT / 'include').glob('*.h')))
     return sorted(set(re.findall(r'\b(lbf_[a-z_]+)\s*\(', text)))
 
 
