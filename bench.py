@@ -220,10 +220,18 @@ def main():
                     help='mlups: the throughput line; ttp: time to permeability, plain FP64 vs reduced storage')
     ap.add_argument('--storages', default='fp64,bfp16,fp16,fp32')
     ap.add_argument('--max-steps', type=int, default=400000)
-    ap.add_argument('--workload', default='scsp', choices=('scsp', 'color', 'batch'),
+    ap.add_argument('--workload', default='scsp', choices=('scsp', 'color', 'batch', 'operator'),
                     help='scsp: 256^3 single-phase cube; color: 128x128x256 two-phase color-gradient MRT; '
-                         'batch: many uneven geometries in one launch')
+                         'batch: many uneven geometries in one launch; operator: the warm-start network '
+                         '(forward + backward) on the tensor cores')
     ap.add_argument('--count', type=int, default=512, help='batch: number of geometries')
+    ap.add_argument('--ttp-media', default='cube', choices=('cube', 'eval192'),
+                    help='ttp: the 256^3 cube, or held-out 192^3 media')
+    ap.add_argument('--seeds', type=int, default=8, help='ttp eval192: number of media')
+    ap.add_argument('--report', type=int, default=1000, help='ttp: report interval in steps')
+    ap.add_argument('--block', type=int, default=8, help='ttp: block edge of the warm start\'s Darcy correction')
+    ap.add_argument('--warm-weights', default=str(Path(__file__).resolve().parent / 'lbflow_b200' / 'weights' /
+                                                  'warmstart.pt'), help='ttp: trained warm-start operator')
     ap.add_argument('--check', type=int, default=8, help='batch: geometries re-solved alone in FP64')
     args = ap.parse_args()
     if args.warmup < 3:
@@ -236,6 +244,8 @@ def main():
         return color_throughput(args)
     if args.workload == 'batch':
         return batch_run(args)
+    if args.workload == 'operator':
+        return operator_run(args)
 
     import torch
     import torch.distributed as dist
@@ -431,44 +441,156 @@ def batch_run(args):
     return 0
 
 
+def ttp_media(args):
+    """Media of the time-to-permeability runs: the 256^3 cube of the MLUPS line
+    (sigma 3, porosity 0.22), or --ttp-media eval192: 192^3 media with
+    sigma ~ U[2, 5] and porosity ~ U[0.15, 0.30] from seeds that no training
+    medium uses."""
+    if args.ttp_media == 'cube':
+        return [dict(name=f'cube{args.size}', geometry=make_geometry(args.size, 3.0, 0.22, seed=0),
+                     sigma=3.0, porosity=0.22, seed=0)]
+    out = []
+    for k in range(args.seeds):
+        seed = 900000 + k
+        rng = np.random.default_rng([seed, 5])
+        sigma, por = float(rng.uniform(2.0, 5.0)), float(rng.uniform(0.15, 0.30))
+        out.append(dict(name=f'eval192_{k}', geometry=make_geometry(192, sigma, por, seed=seed), sigma=sigma,
+                        porosity=por, seed=seed))
+    return out
+
+
 def time_to_permeability(args):
     """Wall time to LBFlow's convergence criterion (report every 1000 steps,
-    relative velocity change < 1e-6 three times in a row) for the plain FP64
-    path and each reduced-precision storage, with K = nu <u_x> / g and its
-    error against the FP64 result."""
+    relative velocity change < 1e-6 three times in a row) and to K within 1e-3
+    of the plain FP64 result, for each run of --storages: a storage name
+    (fp64, fp32, fp16, bf16, bfp16) starts from rest as LBFlow does; a
+    '+warm' suffix starts from the learned warm start (feature computation,
+    network inference and the coarse Darcy pressure correction with --block
+    voxel blocks inside the timed region); '+warmB' sets the block edge B
+    (0: network only).  K = nu <u_x> / g."""
     import torch
     from lbflow_b200 import Engine
     from lbflow_b200.permeability import converge, time_to_band
     torch.cuda.set_device(0)
-    geometry = make_geometry(args.size, 3.0, 0.22, seed=0)
-    runs = {}
-    hist = {}
-    for storage in args.storages.split(','):
-        eng = Engine(geometry, LABELS, model='scsp', collision=args.collision, tau=(1.0,), rho=(1.0,),
-                     storage=storage)
-        r = converge(eng, 1.0, 1e-5, report=1000, tol=1e-6, max_steps=args.max_steps)
-        hist[storage] = r['history']
-        runs[storage] = dict(steps=r['steps'], seconds=r['seconds'], K=r['K'], converged=r['converged'],
-                             fluid_nodes=eng.fluid_nodes,
-                             mlups=eng.fluid_nodes * r['steps'] / r['seconds'] / 1e6)
-        eng.close()
-    base = runs.get('fp64')
-    for k, v in runs.items():
-        if base:
-            v['K_rel_error_vs_fp64'] = abs(v['K'] - base['K']) / abs(base['K'])
-            v['speedup_vs_fp64'] = base['seconds'] / v['seconds']
-            band = time_to_band(hist[k], base['K'], 1e-3)
-            v['to_1e-3_band'] = dict(steps=band[0], seconds=band[1]) if band else None
-    if base and runs['fp64'].get('to_1e-3_band'):
-        b0 = runs['fp64']['to_1e-3_band']['seconds']
+    net = None
+    if any('+warm' in r for r in args.storages.split(',')):
+        from lbflow_b200 import warmstart as ws
+        net, wmeta = ws.load(args.warm_weights)
+    media = ttp_media(args)
+    results = []
+    for med in media:
+        geometry = med['geometry']
+        fluid = torch.from_numpy(geometry != 255).cuda()
+        runs, hist = {}, {}
+        for name in args.storages.split(','):
+            storage, _, warm = name.partition('+')
+            block = int(warm[4:]) if warm[4:] else args.block
+            eng = Engine(geometry, LABELS, model='scsp', collision=args.collision, tau=(1.0,), rho=(1.0,),
+                         storage=storage)
+            start = (lambda: ws.warm_start(eng, net, fluid, 1.0, 1e-5, block=block)) if warm else None
+            r = converge(eng, 1.0, 1e-5, report=args.report, tol=1e-6, max_steps=args.max_steps, warm=start)
+            hist[name] = r['history']
+            runs[name] = dict(steps=r['steps'], seconds=r['seconds'], K=r['K'], converged=r['converged'],
+                              fallback=r['fallback'], fluid_nodes=eng.fluid_nodes,
+                              mlups=eng.fluid_nodes * r['steps'] / r['seconds'] / 1e6)
+            eng.close()
+        base = runs.get('fp64')
         for k, v in runs.items():
-            if v.get('to_1e-3_band'):
-                v['to_1e-3_band']['speedup_vs_fp64'] = b0 / v['to_1e-3_band']['seconds']
-    print(json.dumps(dict(metric='time to permeability (1e-6 convergence, K within 1e-3 of FP64)',
-                          workload=f'D3Q19 {args.collision} porous cube {args.size}^3, porosity 0.22, sigma 3, '
-                                   f'tau 1, g_x 1e-5', runs=runs)))
+            if base:
+                v['K_rel_error_vs_fp64'] = abs(v['K'] - base['K']) / abs(base['K'])
+                v['speedup_vs_fp64'] = base['seconds'] / v['seconds']
+                band = time_to_band(hist[k], base['K'], 1e-3)
+                v['to_1e-3_band'] = dict(steps=band[0], seconds=band[1]) if band else None
+        if base and runs['fp64'].get('to_1e-3_band'):
+            b0 = runs['fp64']['to_1e-3_band']['seconds']
+            for k, v in runs.items():
+                if v.get('to_1e-3_band'):
+                    v['to_1e-3_band']['speedup_vs_fp64'] = b0 / v['to_1e-3_band']['seconds']
+        results.append(dict(medium=med['name'], sigma=med['sigma'], porosity=med['porosity'], seed=med['seed'],
+                            runs=runs))
+        print(json.dumps(results[-1]), flush=True)
+    summary = {}
+    for name in args.storages.split(','):
+        sp = [r['runs'][name]['to_1e-3_band']['speedup_vs_fp64'] for r in results
+              if r['runs'][name].get('to_1e-3_band') and 'speedup_vs_fp64' in r['runs'][name]['to_1e-3_band']]
+        ke = [r['runs'][name].get('K_rel_error_vs_fp64') for r in results if 'K_rel_error_vs_fp64' in r['runs'][name]]
+        summary[name] = dict(band_speedup_median=float(np.median(sp)) if sp else None,
+                             band_speedup_min=float(min(sp)) if sp else None,
+                             K_rel_error_max=float(max(ke)) if ke else None,
+                             fallbacks=sum(bool(r['runs'][name]['fallback']) for r in results))
+    print(json.dumps(dict(metric='time to permeability (K within 1e-3 of converged FP64; 1e-6 convergence)',
+                          media=args.ttp_media, report_interval=args.report,
+                          workload=f'D3Q19 {args.collision}, tau 1, g_x 1e-5, periodic porous media',
+                          summary=summary)))
     return 0
 
+
+
+def operator_run(args):
+    """Training step of the warm-start operator: forward + backward of the
+    4-level U-Net on a batch of 2 x 96^3 media, every convolution on the
+    tcgen05 kernels.  value = model TFLOP/s (3 x forward FLOPs per step).
+    The roofline line is for the heaviest single convolution launch (the
+    64-channel 3x3x3 periodic convolution at 2 x 48^3, forward), timed per
+    launch with CUDA events and compared with the measured bf16 peak."""
+    import torch
+    from lbflow_b200 import conv
+    from lbflow_b200 import warmstart as ws
+    torch.cuda.set_device(0)
+    d = json.loads((ROOT / 'MEASURED_PEAKS.json').read_text()) if (ROOT / 'MEASURED_PEAKS.json').exists() else {}
+    peak = float(d.get('bf16_tflops', 1590.0))
+    net = ws.WarmStartNet(seed=0).cuda()
+    rng = np.random.default_rng(0)
+    fl = torch.from_numpy(rng.random((2, 96, 96, 96)) < 0.3).cuda()
+    x = ws.features(fl)
+    R = torch.randn(2, 96, 96, 96, 8, device='cuda').to(torch.bfloat16)
+    flops = 3 * net.flops(96 ** 3) * 2
+
+    def step():
+        net.zero_grad(set_to_none=True)
+        y = net(x)
+        (y.float() * R.float()).sum().backward()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    steps = max(5, min(args.steps, 50))
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clocks:
+        t0.record()
+        for _ in range(steps):
+            step()
+        t1.record()
+        torch.cuda.synchronize()
+    conv.check()
+    ms = t0.elapsed_time(t1) / steps
+    # Heaviest single launch: 64 -> 64 channel 3x3x3 conv at 2 x 48^3 (level 3 of a 192^3 input).
+    xa = torch.randn(2, 48, 48, 48, 64, device='cuda').to(torch.bfloat16)
+    w = torch.randn(64, 64, 3, 3, 3, device='cuda') * 0.05
+    b = torch.zeros(64, device='cuda')
+    lf = 2 * 2 * 48 ** 3 * 27 * 64 * 64
+    for _ in range(3):
+        conv.conv3(xa, w, b, 0.1)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(20)]
+    for a, c in ev:
+        a.record()
+        conv.conv3(xa, w, b, 0.1)
+        c.record()
+    torch.cuda.synchronize()
+    conv.check()
+    launch_ms = statistics.fmean(a.elapsed_time(c) for a, c in ev)
+    achieved = lf / (launch_ms / 1e3) / 1e12
+    print(json.dumps(dict(metric='warm-start operator training step, model TFLOP/s', value=flops / (ms / 1e3) / 1e12,
+                          unit='TFLOP/s', steps=steps, warmup=args.warmup, ms_per_step=ms, higher_is_better=True,
+                          dtype='bf16 (fp32 accumulate)', data='synthetic',
+                          config=dict(workload='4-level U-Net, 2 x 96^3 media, forward + backward',
+                                      params=sum(p.numel() for p in net.parameters()), flops_per_step=flops),
+                          roofline=dict(bound='tensor', achieved=achieved, peak=peak, unit='TFLOP/s',
+                                        frac=achieved / peak, traffic=None, peak_kind='measured burst bf16',
+                                        kernel='igemm conv3 64->64 at 2x48^3 (forward)', launch_ms=launch_ms),
+                          gpu_launches=None, clocks=clocks.summary())))
+    return 0
 
 def end_to_end(geometry, args, device):
     """Same metric through the C ABI with host buffers: geometry upload and

@@ -110,7 +110,8 @@ void lbf_destroy(lbf_engine *e);
 
 /* The t = 0 stage of Run: initialize, calcMacroVar, bodyForce and the initial
  * collision (scsp.cpp:60-71, 116-134; colorfluid.cpp:123-138, 214-236).  The
- * t = 0 macroscopic fields are kept for lbf_get_macros. */
+ * t = 0 macroscopic fields are kept for lbf_get_macros.  The device error
+ * word is cleared first, so an engine can be restarted after an error. */
 int lbf_initialize(lbf_engine *e);
 
 /* Warm start (single-phase only): as lbf_initialize, but the t = 0
@@ -118,8 +119,10 @@ int lbf_initialize(lbf_engine *e);
  * rest.  fields: DEVICE memory on the engine's device, one record of `ld`
  * floats (ld >= 4) per voxel in (z, y, x) order, x fastest: velocity x, y, z
  * (the macroscopic velocity, half force included) and density.  Solid voxels
- * are ignored.  The read happens on the engine's stream; the caller keeps
- * the array alive until lbf_synchronize or any blocking call returns.
+ * are ignored.  The call first waits for all work queued on the device, so
+ * fields written on any stream are complete; the read then happens on the
+ * engine's stream and the caller keeps the array alive until lbf_synchronize
+ * or any blocking call returns.
  * flags: reserved, 0. */
 int lbf_initialize_equilibrium(lbf_engine *e, const float *fields, uint32_t ld, uint32_t flags);
 

@@ -633,6 +633,8 @@ int lbf_initialize(lbf_engine* e)
     if (!e) return fail(e, LBF_EINVAL, "NULL engine");
     int rc = setdev(e);
     if (rc) return rc;
+    // A fresh t = 0 state starts with a clear device error word.
+    LBF_CK(e, cudaMemsetAsync(e->err, 0, sizeof(uint32_t), e->stream));
     const Grid g = grid_of(e);
     if (e->cfg.model == LBF_MODEL_SCSP)
         launch_scsp_init(e->D, (int)e->cfg.storage, g, e->force, e->cfg.rho[0], e->f[e->cur], e->ex[e->cur],
@@ -652,12 +654,17 @@ int lbf_initialize_equilibrium(lbf_engine* e, const float* fields, uint32_t ld, 
     if (e->cfg.model != LBF_MODEL_SCSP) return fail(e, LBF_EINVAL, "equilibrium initialisation is single-phase only");
     int rc = setdev(e);
     if (rc) return rc;
+    // The fields usually come from another stream (an inference framework's,
+    // or a copy from pageable memory that returns before its DMA lands):
+    // wait for all queued device work so the read below sees them complete.
+    LBF_CK(e, cudaDeviceSynchronize());
     cudaPointerAttributes pa{};
     if (cudaPointerGetAttributes(&pa, fields) != cudaSuccess || pa.type != cudaMemoryTypeDevice ||
         pa.device != e->cfg.device) {
         cudaGetLastError();
         return fail(e, LBF_EINVAL, "fields must be device memory of the engine's device");
     }
+    LBF_CK(e, cudaMemsetAsync(e->err, 0, sizeof(uint32_t), e->stream));
     const Grid g = grid_of(e);
     launch_scsp_init_eq(e->D, (int)e->cfg.storage, g, e->force, e->cfg.rho[0], fields, ld, e->f[e->cur],
                         e->ex[e->cur], e->stream);

@@ -48,6 +48,38 @@ def porous_medium(shape, sigma, porosity, seed):
     return _largest_periodic_cluster(fluid)
 
 
+def percolates(fluid, axis=-1):
+    """True if a fluid path crosses the box from face to face along `axis`
+    (x by default), with the other two axes periodic: the geometry then
+    carries a non-zero flux under a body force along that axis."""
+    from scipy import ndimage as ndi
+    axis = axis % fluid.ndim
+    lab, n = ndi.label(fluid)
+    if n == 0:
+        return False
+    parent = np.arange(n + 1)
+
+    def find(a):
+        while parent[a] != a:
+            parent[a] = parent[parent[a]]
+            a = parent[a]
+        return a
+
+    for ax in range(fluid.ndim):
+        if ax == axis:
+            continue
+        a = np.take(lab, 0, axis=ax)
+        b = np.take(lab, -1, axis=ax)
+        m = (a > 0) & (b > 0)
+        for u, v in set(zip(a[m].tolist(), b[m].tolist())):
+            ru, rv = find(u), find(v)
+            if ru != rv:
+                parent[ru] = rv
+    lo = {find(int(v)) for v in np.unique(np.take(lab, 0, axis=axis)) if v}
+    hi = {find(int(v)) for v in np.unique(np.take(lab, -1, axis=axis)) if v}
+    return bool(lo & hi)
+
+
 def labels_from_mask(fluid, fluid_label=75, solid_label=255):
     return np.where(fluid, fluid_label, solid_label).astype(np.uint8)
 

@@ -22,10 +22,24 @@ def permeability(engine, tau, g, axis=0):
 
 
 def converge(engine, tau, g, report=1000, tol=1e-6, max_steps=2_000_000, initialized=False,
-             on_report=None):
+             on_report=None, warm=None, patience=5, t0=None):
     """Step to the reference's convergence criterion; returns a dict with the
-    completed steps, wall seconds (device work included), K and the residual history."""
-    if not initialized:
+    completed steps, wall seconds (device work included), K and the residual history.
+
+    warm: optional callable that initialises the engine (a warm start).  The
+    run then falls back to LBFlow's start from rest (engine.initialize) when
+    the warm-started residual is non-finite, the device reports a numerical
+    error, or the residual, still above 100 * tol, sets no new minimum for
+    `patience` reports.  Steps
+    and seconds count both attempts; `fallback` in the result says whether it
+    happened.  t0: perf_counter value the seconds count from (default: the
+    start of this call, after the engine's queued work)."""
+    engine.synchronize()
+    if t0 is None:
+        t0 = time.perf_counter()
+    if warm is not None:
+        warm()
+    elif not initialized:
         engine.initialize()
     D = engine.dims
     count = D * engine.N
@@ -33,13 +47,27 @@ def converge(engine, tau, g, report=1000, tol=1e-6, max_steps=2_000_000, initial
     stable = 0
     first = True
     history = []
-    engine.synchronize()
-    t0 = time.perf_counter()
+    warm_active = warm is not None
+    fallback = False
+    best, since_best = math.inf, 0
+
+    def restart():
+        nonlocal first, stable, warm_active, fallback, best, since_best
+        engine.initialize()
+        first, stable, warm_active, fallback = True, 0, False, True
+        best, since_best = math.inf, 0
+
     while t < max_steps:
         engine.step(report - 1, adjacent=True)
         engine.step(1, macros=True)
         t += report
-        engine.check()
+        try:
+            engine.check()
+        except Exception:
+            if not warm_active:
+                raise
+            restart()
+            continue
         K = permeability(engine, tau, g)
         if first:
             engine.convergence(first=True)
@@ -48,6 +76,9 @@ def converge(engine, tau, g, report=1000, tol=1e-6, max_steps=2_000_000, initial
             continue
         s = engine.convergence()
         if not all(math.isfinite(v) for v in s[:3]):
+            if warm_active:
+                restart()
+                continue
             raise RuntimeError('Invalid global velocity residual.')
         rms = math.sqrt(s[0] / count)
         res = math.sqrt(s[0] / s[1]) if s[1] > 0 else 0.0
@@ -60,10 +91,19 @@ def converge(engine, tau, g, report=1000, tol=1e-6, max_steps=2_000_000, initial
             on_report(t, res, ares)
         if stable >= 3:
             break
+        if res < best:
+            best, since_best = res, 0
+        else:
+            since_best += 1
+        # A stall far above the tolerance means the warm start went wrong; near
+        # the tolerance it is the storage precision's floor, which a restart
+        # would not change.
+        if warm_active and since_best >= patience and best > 100 * tol:
+            restart()
     engine.synchronize()
     seconds = time.perf_counter() - t0
     return dict(steps=t, seconds=seconds, K=permeability(engine, tau, g), converged=stable >= 3,
-                history=history)
+                history=history, fallback=fallback)
 
 
 def time_to_band(history, K_ref, rel=1e-3):

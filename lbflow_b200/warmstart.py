@@ -1,0 +1,385 @@
+"""Learned warm start: a 3D convolutional neural operator that predicts the
+steady flow of a periodic porous medium under a body force, used as the
+initial state of the lattice Boltzmann run.
+
+LBFlow always starts from rest (SCSP::initialize, solver/src/lbm/scsp.cpp:
+116-134) and steps until its velocity residual falls below stopError
+(Simulator::updateConvergence, simulator.cpp:248-325).  Here the network maps
+the voxel geometry to the steady velocity and density; the engine starts from
+the equilibrium populations of that prediction (lbf_initialize_equilibrium)
+and the unchanged step loop and stopping rule take it from there, so the
+converged answer is the solver's, not the network's.  If the residual stalls
+or blows up the run restarts from rest (the cold-start fallback).
+
+Scaling.  In the creeping-flow regime of these runs (Re << 1) the steady
+velocity is linear in the force: u = (g / nu) k(x) with nu = (tau - 1/2)/3,
+and the density deviation is rho - rho0 = 3 g pi(x).  The network predicts
+the geometry-only fields k (whose mean over all voxels is the permeability K
+of scripts/rock_workflow.py:60-66) and pi, normalised by constants stored
+with the weights, so one network serves every tau and force magnitude.  The
+force must lie along +x; other directions are handled by the caller
+permuting axes.
+
+Network (about 1.8M parameters, bf16 activations, fp32 master weights):
+a 4-level U-Net on channels-last tensors whose every convolution, data
+gradient and weight gradient runs in the tcgen05 kernels of conv.py.
+Channels 16-32-64-128; per level two periodic 3x3x3 convolutions with leaky
+ReLU, 2x2x2 stride-2 convolutions down, 2x2x2 stride-2 transposed
+convolutions up, skip connections concatenated inside the decoder's first
+convolution, and a linear 3x3x3 head.  Grid edges must be multiples of 8.
+"""
+import math
+import time
+
+import numpy as np
+import torch
+
+from . import conv
+
+CH = (16, 32, 64, 128)
+IN_CH = 8          # input features (5 used, zero padded to a multiple of 8)
+OUT_CH = 8         # head channels: k_x, k_y, k_z, pi, 4 unused
+SLOPE = 0.1
+DIST_MAX = 12      # chessboard distances are capped here
+
+
+def _spec():
+    c1, c2, c3, c4 = CH
+    s = [('enc1a', 'c3', IN_CH, c1), ('enc1b', 'c3', c1, c1), ('down1', 'd2', c1, c2),
+         ('enc2a', 'c3', c2, c2), ('enc2b', 'c3', c2, c2), ('down2', 'd2', c2, c3),
+         ('enc3a', 'c3', c3, c3), ('enc3b', 'c3', c3, c3), ('down3', 'd2', c3, c4),
+         ('mida', 'c3', c4, c4), ('midb', 'c3', c4, c4),
+         ('up3', 'u2', c4, c3), ('dec3a', 'c3', 2 * c3, c3), ('dec3b', 'c3', c3, c3),
+         ('up2', 'u2', c3, c2), ('dec2a', 'c3', 2 * c2, c2), ('dec2b', 'c3', c2, c2),
+         ('up1', 'u2', c2, c1), ('dec1a', 'c3', 2 * c1, c1), ('dec1b', 'c3', c1, c1),
+         ('head', 'c3', c1, OUT_CH)]
+    return s
+
+
+class WarmStartNet(torch.nn.Module):
+    def __init__(self, seed=0):
+        super().__init__()
+        g = torch.Generator().manual_seed(seed)
+        self.kinds = {}
+        for name, kind, cin, cout in _spec():
+            if kind == 'u2':
+                w = torch.randn(cin, cout, 2, 2, 2, generator=g) * math.sqrt(2.0 / cin)
+            else:
+                k = 3 if kind == 'c3' else 2
+                w = torch.randn(cout, cin, k, k, k, generator=g) * math.sqrt(2.0 / (cin * k ** 3))
+            if name == 'head':
+                w *= 0.1
+            self.register_parameter(name + '_w', torch.nn.Parameter(w))
+            self.register_parameter(name + '_b', torch.nn.Parameter(torch.zeros(cout)))
+            self.kinds[name] = kind
+        # Normalisation of the targets (set from the training data).
+        self.register_buffer('scale', torch.ones(4))
+
+    def _p(self, name):
+        return getattr(self, name + '_w'), getattr(self, name + '_b')
+
+    def _c3(self, name, x, skip=None, act=True):
+        w, b = self._p(name)
+        return conv.conv3(x, w, b, SLOPE if act else None, x1=skip)
+
+    def forward(self, x):
+        """x: (B, D, H, W, 8) bf16 features -> (B, D, H, W, 8) bf16 outputs."""
+        e1 = self._c3('enc1b', self._c3('enc1a', x))
+        e2 = conv.down2(e1, *self._p('down1'), SLOPE)
+        e2 = self._c3('enc2b', self._c3('enc2a', e2))
+        e3 = conv.down2(e2, *self._p('down2'), SLOPE)
+        e3 = self._c3('enc3b', self._c3('enc3a', e3))
+        m = conv.down2(e3, *self._p('down3'), SLOPE)
+        m = self._c3('midb', self._c3('mida', m))
+        d3 = conv.up2(m, *self._p('up3'), SLOPE)
+        d3 = self._c3('dec3b', self._c3('dec3a', d3, skip=e3))
+        d2 = conv.up2(d3, *self._p('up2'), SLOPE)
+        d2 = self._c3('dec2b', self._c3('dec2a', d2, skip=e2))
+        d1 = conv.up2(d2, *self._p('up1'), SLOPE)
+        d1 = self._c3('dec1b', self._c3('dec1a', d1, skip=e1))
+        return self._c3('head', d1, act=False)
+
+    def flops(self, voxels):
+        """Forward FLOPs (2 x multiply-adds) of one sample of `voxels` voxels."""
+        total = 0
+        level = {'enc1': 1, 'dec1': 1, 'enc2': 8, 'dec2': 8, 'enc3': 64, 'dec3': 64, 'mid': 512,
+                 'down1': 8, 'down2': 64, 'down3': 512, 'up3': 512, 'up2': 64, 'up1': 8, 'head': 1}
+        for name, kind, cin, cout in _spec():
+            key = next(k for k in level if name.startswith(k))
+            rows = voxels / level[key]
+            taps = {'c3': 27, 'd2': 8, 'u2': 8}[kind]
+            total += 2 * rows * taps * cin * cout
+        return total
+
+
+def _periodic_pool(x, k, mode):
+    p = k // 2
+    xp = torch.nn.functional.pad(x, (p, p, p, p, p, p), mode='circular')
+    if mode == 'max':
+        return torch.nn.functional.max_pool3d(xp, k, stride=1)
+    return torch.nn.functional.avg_pool3d(xp, k, stride=1)
+
+
+def features(fluid):
+    """Input features of (B, D, H, W) fluid masks (bool or 0/1, any device):
+    mask, signed chessboard distance / 8 (positive in pores), its squared
+    positive part / 64, porosity of the surrounding 9^3 box, global porosity.
+    Returns (B, D, H, W, 8) bf16, channels-last, on the masks' device."""
+    m = fluid.float().unsqueeze(1)                      # (B, 1, D, H, W)
+    solid = 1.0 - m
+    dist_f = torch.zeros_like(m)
+    dist_s = torch.zeros_like(m)
+    cur_s, cur_f = solid, m
+    for _ in range(DIST_MAX):
+        dist_f += 1.0 - cur_s                           # pores not yet reached by the dilated solid
+        dist_s += 1.0 - cur_f
+        cur_s = _periodic_pool(cur_s, 3, 'max')
+        cur_f = _periodic_pool(cur_f, 3, 'max')
+    sdf = (dist_f - dist_s) / 8.0
+    por = _periodic_pool(m, 9, 'avg')
+    glob = m.mean(dim=(2, 3, 4), keepdim=True).expand_as(m)
+    z = torch.zeros_like(m)
+    f = torch.cat([m, sdf, torch.clamp(sdf, min=0) ** 2, por, glob, z, z, z], dim=1)
+    return f.permute(0, 2, 3, 4, 1).contiguous().to(torch.bfloat16)
+
+
+def targets(rho, u, tau, g, rho0=1.0):
+    """Geometry-only fields of a steady solution: k = u nu / g (3 components)
+    and pi = (rho - rho0) / (3 g), stacked as (D, H, W, 4) float32."""
+    nu = (tau - 0.5) / 3.0
+    k = np.moveaxis(u, 0, -1) * (nu / g)
+    pi = (rho - rho0) / (3.0 * g)
+    pi = np.where(rho > 0, pi, 0.0)
+    return np.concatenate([k, pi[..., None]], axis=-1).astype(np.float32)
+
+
+def _block_mean(x, b):
+    """Means over b^3 blocks of a (D, H, W, C) field -> (D/b, H/b, W/b, C)."""
+    D, H, W, C = x.shape
+    return x.reshape(D // b, b, H // b, b, W // b, b, C).mean(dim=(1, 3, 5))
+
+
+def _shift(x, s, axis):
+    return torch.roll(x, s, dims=axis)
+
+
+def darcy_pressure(q, mob, b, iters=400, rtol=1e-10):
+    """Coarse pressure that makes a block-averaged flux field conservative.
+
+    q: (d, h, w, 3) block-mean velocity (x, y, z) of a periodic medium;
+    mob: (d, h, w) block mobility (flux per unit driving force); b: block
+    edge in voxels.  Face fluxes are the means of the two blocks' fluxes and
+    face mobilities the harmonic means of their mobilities (series layers).
+    Solves  sum_faces M_f (phi_nb - phi) / b^2 = div q  with periodic wrap by
+    conjugate gradients preconditioned with the mean-mobility Laplacian
+    (inverted by FFT), so that  q - M grad(phi)  has zero divergence.
+    phi is the pressure over rho0 (p / rho0), zero mean.  FP64 throughout."""
+    q = q.double()
+    mob = mob.double().clamp(min=1e-30)
+    axes = (2, 1, 0)            # x, y, z components live on grid axes W, H, D
+    div = torch.zeros_like(mob)
+    mf = []
+    for c, ax in enumerate(axes):
+        flux = 0.5 * (q[..., c] + _shift(q[..., c], -1, ax))          # face i + 1/2
+        div += (flux - _shift(flux, 1, ax)) / b
+        nb = _shift(mob, -1, ax)
+        mf.append(2.0 * mob * nb / (mob + nb))
+
+    def A(phi):
+        out = torch.zeros_like(phi)
+        for c, ax in enumerate(axes):
+            grad = (_shift(phi, -1, ax) - phi) / b                   # at face i + 1/2
+            f = mf[c] * grad
+            out += (f - _shift(f, 1, ax)) / b
+        return out
+
+    d, h, w = mob.shape
+    kz = torch.fft.fftfreq(d, dtype=torch.float64, device=mob.device)
+    ky = torch.fft.fftfreq(h, dtype=torch.float64, device=mob.device)
+    kx = torch.fft.fftfreq(w, dtype=torch.float64, device=mob.device)
+    lap = sum((2.0 * torch.cos(2 * math.pi * k) - 2.0) / b ** 2 for k in
+              (kz[:, None, None], ky[None, :, None], kx[None, None, :]))
+    mbar = torch.stack(mf).mean()
+    inv = torch.where(lap.abs() > 0, 1.0 / (mbar * lap), torch.zeros_like(lap))
+
+    def M(r):
+        return torch.fft.ifftn(torch.fft.fftn(r) * inv).real
+
+    rhs = div - div.mean()
+    phi = torch.zeros_like(rhs)
+    r = rhs.clone()
+    z = M(r)
+    p = z.clone()
+    rz = (r * z).sum()
+    nrm = rhs.norm()
+    if nrm == 0:
+        return phi
+    for _ in range(iters):
+        Ap = A(p)
+        alpha = rz / (p * Ap).sum()
+        phi = phi + alpha * p
+        r = r - alpha * Ap
+        if r.norm() <= rtol * nrm:
+            break
+        z = M(r)
+        rz_new = (r * z).sum()
+        p = z + (rz_new / rz) * p
+        rz = rz_new
+    return phi - phi.mean()
+
+
+def _upsample_periodic(phi, b):
+    """Trilinear interpolation of block-centre values to voxel centres, periodic."""
+    x = phi[None, None]
+    x = torch.nn.functional.pad(x, (1, 1, 1, 1, 1, 1), mode='circular')
+    d, h, w = phi.shape
+    up = torch.nn.functional.interpolate(x, scale_factor=b, mode='trilinear', align_corners=False)
+    # Padding by one block shifts the interpolated grid by b voxels.
+    return up[0, 0, b:b + d * b, b:b + h * b, b:b + w * b]
+
+
+def coarse_correction(u, fluid, g, block=8):
+    """Density correction (per voxel) that removes the large-scale mass
+    imbalance of a predicted velocity field u (D, H, W, 3) under force g
+    along +x: block fluxes and mobilities from u, darcy_pressure, interpolated
+    to the voxels and converted to density (rho = 3 p at c_s^2 = 1/3)."""
+    b = block
+    q = _block_mean(u.double(), b)
+    mob = q[..., 0] / g
+    mob = torch.clamp(mob, min=1e-3 * float(mob.clamp(min=0).mean()) + 1e-30)
+    phi = darcy_pressure(q, mob, b)
+    return 3.0 * _upsample_periodic(phi, b) * fluid.double()
+
+
+def predict(net, fluid, tau, g, rho0=1.0, block=8):
+    """Warm-start fields (D, H, W, 4) float32 on the GPU: velocity x, y, z and
+    density for force g along +x and relaxation time tau.  block: edge of
+    the coarse Darcy correction (0 = network only)."""
+    with torch.no_grad():
+        f = features(fluid.unsqueeze(0))
+        y = net(f)[0, ..., :4].float() * net.scale
+        m = fluid.float()
+        nu = (tau - 0.5) / 3.0
+        out = torch.empty(*fluid.shape, 4, dtype=torch.float32, device=fluid.device)
+        out[..., :3] = y[..., :3] * (g / nu) * m[..., None]
+        drho = 3.0 * g * y[..., 3].double() * m
+        if block:
+            drho = drho + coarse_correction(out[..., :3], fluid, g, block)
+        # Zero-mean density deviation over the pores (mass of the rest state).
+        drho = drho - drho.sum() / m.sum().clamp(min=1.0) * m
+        out[..., 3] = (rho0 + drho).float()
+        conv.check(fluid.device)
+        return out.contiguous()
+
+
+def warm_start(engine, net, fluid, tau, g, rho0=1.0, block=8):
+    """Initialise `engine` from the network's prediction; returns the fields."""
+    fields = predict(net, fluid, tau, g, rho0, block)
+    torch.cuda.current_stream(fluid.device).synchronize()
+    engine.initialize_equilibrium(fields.data_ptr(), 4)
+    return fields
+
+
+def save(net, path, meta=None):
+    torch.save({'state': {k: v.detach().cpu() for k, v in net.state_dict().items()}, 'ch': CH,
+                'meta': meta or {}}, path)
+
+
+def load(path, device='cuda'):
+    ck = torch.load(path, map_location='cpu', weights_only=False)
+    if tuple(ck['ch']) != CH:
+        raise ValueError(f'weights are for channels {ck["ch"]}, this network has {CH}')
+    net = WarmStartNet()
+    net.load_state_dict(ck['state'])
+    return net.to(device), ck.get('meta', {})
+
+
+# ----------------------------------------------------------------- training --
+
+def _augment(feat, targ, gen):
+    """Random periodic shift, y/z mirrors and the y<->z swap (symmetries of a
+    periodic medium under a force along x)."""
+    dims = feat.shape[1:4]
+    shifts = [int(torch.randint(0, d, (1,), generator=gen)) for d in dims]
+    feat = torch.roll(feat, shifts, dims=(1, 2, 3))
+    targ = torch.roll(targ, shifts, dims=(1, 2, 3))
+    if torch.rand(1, generator=gen).item() < 0.5:          # mirror z: k_z -> -k_z
+        feat, targ = feat.flip(1), targ.flip(1)
+        targ = targ * torch.tensor([1, 1, -1, 1.0], device=targ.device)
+    if torch.rand(1, generator=gen).item() < 0.5:          # mirror y: k_y -> -k_y
+        feat, targ = feat.flip(2), targ.flip(2)
+        targ = targ * torch.tensor([1, -1, 1, 1.0], device=targ.device)
+    if dims[0] == dims[1] and torch.rand(1, generator=gen).item() < 0.5:   # swap z and y
+        feat = feat.transpose(1, 2)
+        targ = targ.transpose(1, 2)[..., [0, 2, 1, 3]]
+    return feat.contiguous(), targ.contiguous()
+
+
+def train(net, samples, iters=2000, lr=2e-3, batch_voxels=2 * 64 ** 3, seed=0, log=None, weights=(1, 0.5, 0.5, 2)):
+    """samples: list of (fluid mask (D,H,W) bool cuda, target (D,H,W,4) float cuda).
+    Minimises the normalised mean-square error over pore voxels with AdamW and
+    a cosine learning-rate schedule.  Returns the loss history."""
+    dev = samples[0][0].device
+    # Normalisation: RMS of each target channel over pores.
+    num = torch.zeros(4, dtype=torch.float64, device=dev)
+    cnt = 0.0
+    for fl, t in samples:
+        num += (t[fl].double() ** 2).sum(0)
+        cnt += float(fl.sum())
+    scale = torch.sqrt(num / max(cnt, 1.0)).float().clamp(min=1e-6)
+    net.scale.copy_(scale)
+    by_shape = {}
+    for i, (fl, _) in enumerate(samples):
+        by_shape.setdefault(tuple(fl.shape), []).append(i)
+    shapes = sorted(by_shape)
+    feats = [features(fl.unsqueeze(0))[0] for fl, _ in samples]
+    opt = torch.optim.AdamW(net.parameters(), lr=lr, weight_decay=1e-4)
+    gen = torch.Generator().manual_seed(seed)
+    wts = torch.tensor(weights, dtype=torch.float32, device=dev)
+    hist = []
+    t0 = time.perf_counter()
+    for it in range(iters):
+        for gparam in opt.param_groups:
+            gparam['lr'] = lr * 0.5 * (1 + math.cos(math.pi * it / iters))
+        shp = shapes[int(torch.randint(0, len(shapes), (1,), generator=gen))]
+        pool = by_shape[shp]
+        nb = max(1, min(len(pool), batch_voxels // int(np.prod(shp))))
+        pick = [pool[int(j)] for j in torch.randint(0, len(pool), (nb,), generator=gen)]
+        fb, tb = [], []
+        for j in pick:
+            f, t = _augment(feats[j].unsqueeze(0), samples[j][1].unsqueeze(0), gen)
+            fb.append(f)
+            tb.append(t)
+        fb = torch.cat(fb)
+        tb = torch.cat(tb) / scale
+        mask = fb[..., 0].float().unsqueeze(-1)
+        y = net(fb)[..., :4].float()
+        loss = (((y - tb) ** 2) * mask * wts).sum() / (mask.sum() * wts.sum())
+        opt.zero_grad(set_to_none=True)
+        loss.backward()
+        torch.nn.utils.clip_grad_norm_(net.parameters(), 1.0)
+        opt.step()
+        if it % 50 == 0 or it == iters - 1:
+            lv = float(loss)
+            hist.append((it, lv, time.perf_counter() - t0))
+            if log:
+                log(f'iter {it} loss {lv:.4e} shape {shp} batch {nb} {time.perf_counter() - t0:.1f}s')
+    conv.check(dev)
+    return hist
+
+
+def evaluate(net, samples):
+    """Relative L2 error of the predicted k and pi over pores, and of the
+    predicted permeability, per sample."""
+    out = []
+    with torch.no_grad():
+        for fl, t in samples:
+            y = net(features(fl.unsqueeze(0)))[0, ..., :4].float() * net.scale
+            m = fl.float()
+            ek = torch.sqrt((((y[..., :3] - t[..., :3]) ** 2).sum(-1) * m).sum() / ((t[..., :3] ** 2).sum(-1) * m).sum())
+            ep = torch.sqrt((((y[..., 3] - t[..., 3]) ** 2) * m).sum() / ((t[..., 3] ** 2) * m).sum().clamp(min=1e-30))
+            Kp = float((y[..., 0] * m).mean())
+            Kt = float(t[..., 0].mean())
+            out.append(dict(k_rel_l2=float(ek), pi_rel_l2=float(ep), K_pred=Kp, K_true=Kt,
+                            K_rel_err=abs(Kp - Kt) / max(abs(Kt), 1e-30)))
+    return out

@@ -82,3 +82,37 @@ def test_set_get_roundtrip_reduced_precision(storage):
         w = np.array([12] + [2] * 6 + [1] * 12) / 36.0
         dev = np.abs(f - w[None, :, None, None, None])[:, :, fl].max()
         assert np.max(np.abs(g[:, :, fl] - f[:, :, fl])) <= dev * 1e-3 + 1e-9
+
+
+def _color_porous(n=(64, 32, 32), seed=3):
+    from lbflow_b200.geometry import porous_medium
+    fluid = porous_medium(n, sigma=2.0, porosity=0.30, seed=seed)
+    g = np.where(fluid, 76, 255).astype(np.uint8)
+    g[:n[0] // 3][fluid[:n[0] // 3]] = 75
+    labels = {75: ('GV', 2e-6, 5, 0), 76: ('GV', 2e-6, 5, 1), 255: ('SD', 60.0, 0, 0)}
+    return g, labels
+
+
+@pytest.mark.parametrize('steps', [1, 50, 400])
+def test_color_fp32_storage_tracks_fp64(steps):
+    """Two-phase color-gradient run with FP32 populations and arithmetic
+    against FP64: no device error, phase-0 mass and the phase-weighted flux
+    (porous_media.py:33-41) close to FP64."""
+    from lbflow_b200 import Engine
+    g, labels = _color_porous()
+    out = {}
+    for storage in ('fp64', 'fp32'):
+        with Engine(g, labels, model='color', collision='MRT', tau=(1.0, 0.7), rho=(1.0, 1.0), alpha0=1 / 3,
+                    sigma=1e-3, beta=0.7, storage=storage) as e:
+            e.initialize()
+            e.step(steps, macros=True)
+            bits = e.status()
+            r0, r1, u = e.macros()
+            out[storage] = (bits, r0, r1, u)
+    assert out['fp64'][0] == 0
+    assert out['fp32'][0] == 0, f'device error word {out["fp32"][0]:#x}'
+    m64, m32 = out['fp64'][1].sum(), out['fp32'][1].sum()
+    assert abs(m32 - m64) <= 1e-5 * m64
+    du = np.abs(out['fp32'][3] - out['fp64'][3]).max() / max(np.abs(out['fp64'][3]).max(), 1e-30)
+    print(f'steps {steps}: phase-0 mass rel diff {abs(m32 - m64) / m64:.2e}, max |du|/max|u| {du:.2e}')
+    assert du < 1e-2
