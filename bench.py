@@ -230,6 +230,8 @@ def main():
     ap.add_argument('--seeds', type=int, default=8, help='ttp eval192: number of media')
     ap.add_argument('--report', type=int, default=1000, help='ttp: report interval in steps')
     ap.add_argument('--block', type=int, default=8, help='ttp: block edge of the warm start\'s Darcy correction')
+    ap.add_argument('--accel-at', default='1000', help='ttp: report steps at which +acc runs apply the block '
+                                                       'Darcy pressure correction')
     ap.add_argument('--warm-weights', default=str(Path(__file__).resolve().parent / 'lbflow_b200' / 'weights' /
                                                   'warmstart.pt'), help='ttp: trained warm-start operator')
     ap.add_argument('--check', type=int, default=8, help='batch: geometries re-solved alone in FP64')
@@ -465,16 +467,19 @@ def time_to_permeability(args):
     of the plain FP64 result, for each run of --storages: a storage name
     (fp64, fp32, fp16, bf16, bfp16) starts from rest as LBFlow does; a
     '+warm' suffix starts from the learned warm start (feature computation,
-    network inference and the coarse Darcy pressure correction with --block
-    voxel blocks inside the timed region); '+warmB' sets the block edge B
-    (0: network only).  K = nu <u_x> / g."""
+    network inference and the block-scale Darcy pressure with --block voxel
+    blocks, inside the timed region); '+warmB' sets the block edge B (0: the
+    network's fields only); '+fluxB' uses the flux-divergence correction
+    instead; '+accB' applies the in-run block Darcy correction
+    (warmstart.DarcyAccelerator) at the --accel-at report steps.
+    K = nu <u_x> / g."""
     import torch
     from lbflow_b200 import Engine
     from lbflow_b200.permeability import converge, time_to_band
     torch.cuda.set_device(0)
     net = None
-    if any('+warm' in r for r in args.storages.split(',')):
-        from lbflow_b200 import warmstart as ws
+    from lbflow_b200 import warmstart as ws
+    if any('+warm' in r or '+flux' in r for r in args.storages.split(',')):
         net, wmeta = ws.load(args.warm_weights)
     media = ttp_media(args)
     results = []
@@ -483,12 +488,21 @@ def time_to_permeability(args):
         fluid = torch.from_numpy(geometry != 255).cuda()
         runs, hist = {}, {}
         for name in args.storages.split(','):
-            storage, _, warm = name.partition('+')
-            block = int(warm[4:]) if warm[4:] else args.block
+            storage, *mods = name.split('+')
+            start = acc = None
             eng = Engine(geometry, LABELS, model='scsp', collision=args.collision, tau=(1.0,), rho=(1.0,),
                          storage=storage)
-            start = (lambda: ws.warm_start(eng, net, fluid, 1.0, 1e-5, block=block)) if warm else None
-            r = converge(eng, 1.0, 1e-5, report=args.report, tol=1e-6, max_steps=args.max_steps, warm=start)
+            for mod in mods:
+                kind = mod.rstrip('0123456789')
+                block = int(mod[len(kind):]) if mod[len(kind):] else args.block
+                if kind in ('warm', 'flux'):
+                    mode = {'warm': 'darcy', 'flux': 'flux'}[kind] if block else 'none'
+                    start = (lambda b=block, m=mode: ws.warm_start(eng, net, fluid, 1.0, 1e-5, block=b, mode=m))
+                elif kind == 'acc':
+                    acc = ws.DarcyAccelerator(eng, fluid, 1e-5, block=block,
+                                              at=[int(t) for t in args.accel_at.split(',')])
+            r = converge(eng, 1.0, 1e-5, report=args.report, tol=1e-6, max_steps=args.max_steps, warm=start,
+                         accelerate=acc)
             hist[name] = r['history']
             runs[name] = dict(steps=r['steps'], seconds=r['seconds'], K=r['K'], converged=r['converged'],
                               fallback=r['fallback'], fluid_nodes=eng.fluid_nodes,

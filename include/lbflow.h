@@ -126,6 +126,21 @@ int lbf_initialize(lbf_engine *e);
  * flags: reserved, 0. */
 int lbf_initialize_equilibrium(lbf_engine *e, const float *fields, uint32_t ld, uint32_t flags);
 
+/* Sums over block^3 cubes of the fields of the last step that wrote them
+ * (LBF_STEP_MACROS or initialisation), single-phase only.  nx, ny and nz must
+ * be multiples of block (nz = 1 in 2-D is taken as one layer); out: host,
+ * n = (nx/block)(ny/block)(nz/block) * 5 doubles, cube (bz, by, bx) at
+ * ((bz * NBy + by) * NBx + bx) * 5: { sum rho, sum u_x, sum u_y, sum u_z,
+ * fluid voxels } over its fluid voxels, summed in voxel order. */
+int lbf_block_sums(lbf_engine *e, uint32_t block, double *out, size_t n);
+
+/* Adds w_q * drho(voxel) to every population of every fluid node of the
+ * current state: a density change at unchanged momentum (single-phase
+ * only).  drho: DEVICE memory of the engine's device, one float per voxel in
+ * (z, y, x) order; solid voxels are ignored.  Waits for all queued device
+ * work first, like lbf_initialize_equilibrium. */
+int lbf_add_density(lbf_engine *e, const float *drho);
+
 /* nsteps steps of the Run loop body: streaming, bounce-back, calcMacroVar,
  * bodyForce, collision (scsp.cpp:75-104; colorfluid.cpp:142-198).  flags
  * (LBF_STEP_*) apply to the last step of the call. */

@@ -78,6 +78,8 @@ def library():
             'lbf_destroy': (None, [P]),
             'lbf_initialize': (I, [P]),
             'lbf_initialize_equilibrium': (I, [P, P, U32, U32]),
+            'lbf_block_sums': (I, [P, U32, D, ctypes.c_size_t]),
+            'lbf_add_density': (I, [P, P]),
             'lbf_step': (I, [P, U32, U32]),
             'lbf_get_populations': (I, [P, D, ctypes.c_size_t]),
             'lbf_set_populations': (I, [P, D, ctypes.c_size_t]),
@@ -187,10 +189,34 @@ class Engine:
     def initialize(self):
         self._ck(self._lib.lbf_initialize(self._h))
 
-    def initialize_equilibrium(self, fields_ptr, ld=4):
-        """Warm start from device fields: `fields_ptr` is the device address of a
-        dense float32 (z, y, x, ld) array holding velocity x, y, z and density."""
-        self._ck(self._lib.lbf_initialize_equilibrium(self._h, ctypes.c_void_p(int(fields_ptr)), int(ld), 0))
+    def block_sums(self, block):
+        """Per-cube sums of the last written fields: array (NBz, NBy, NBx, 5) of
+        (sum rho, sum u_x, sum u_y, sum u_z, fluid voxels)."""
+        nz, ny, nx = (1,) + tuple(self.shape) if len(self.shape) == 2 else tuple(self.shape)
+        bz = 1 if len(self.shape) == 2 else block
+        shp = (nz // bz, ny // block, nx // block, 5)
+        out = np.zeros(shp)
+        self._ck(self._lib.lbf_block_sums(self._h, int(block), _dptr(out), out.size))
+        return out
+
+    def add_density(self, drho):
+        """Add w_q * drho to the current populations (contiguous float32 CUDA
+        tensor shaped like the geometry): a density change at fixed momentum."""
+        if (tuple(drho.shape) != tuple(self.shape) or str(drho.dtype) != 'torch.float32' or not drho.is_cuda
+                or not drho.is_contiguous()):
+            raise ValueError(f'drho must be a contiguous float32 CUDA tensor of shape {tuple(self.shape)}')
+        self._ck(self._lib.lbf_add_density(self._h, ctypes.c_void_p(drho.data_ptr())))
+
+    def initialize_equilibrium(self, fields):
+        """Warm start from device fields: a contiguous float32 CUDA tensor of
+        shape (nz, ny, nx, ld), ld >= 4, holding velocity x, y, z and density
+        per voxel (2-D grids: (ny, nx, ld))."""
+        shape = tuple(fields.shape)
+        if (shape[:-1] != tuple(self.shape) or shape[-1] < 4 or str(fields.dtype) != 'torch.float32'
+                or not fields.is_cuda or not fields.is_contiguous()):
+            raise ValueError(f'fields must be a contiguous float32 CUDA tensor of shape {tuple(self.shape)} + (>=4,), '
+                             f'got {shape} {fields.dtype} contiguous={fields.is_contiguous()}')
+        self._ck(self._lib.lbf_initialize_equilibrium(self._h, ctypes.c_void_p(fields.data_ptr()), int(shape[-1]), 0))
 
     def step(self, n=1, macros=False, adjacent=False):
         flags = (STEP_MACROS if macros else 0) | (STEP_ADJACENT if adjacent else 0)

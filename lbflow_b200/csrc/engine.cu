@@ -674,6 +674,85 @@ int lbf_initialize_equilibrium(lbf_engine* e, const float* fields, uint32_t ld, 
     return LBF_OK;
 }
 
+namespace {
+// Sums of the macroscopic fields over block^3 cubes: one thread per cube
+// walks its voxels in (z, y, x) order (deterministic).  out[cube * 5 + k] =
+// {sum rho, sum u_x, sum u_y, sum u_z, fluid voxels}.
+__global__ void block_sums_kernel(const lbf::Grid g, const double* __restrict__ rho, const double* __restrict__ u,
+                                  int b, int bx, int by, int bz, double* __restrict__ out)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (uint32_t)(bx * by * bz)) return;
+    const int X0 = (int)(k % bx) * b, Y0 = (int)((k / bx) % by) * b, Z0 = (int)(k / ((uint32_t)bx * by)) * b;
+    double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int z = Z0; z < Z0 + b; ++z)
+        for (int y = Y0; y < Y0 + b; ++y)
+            for (int x = X0; x < X0 + b; ++x) {
+                bool fluid;
+                const uint32_t j = lbf::lookup(g, x, y, z, fluid);
+                if (!fluid) continue;
+                s[0] += rho[j];
+                s[1] += u[j];
+                s[2] += u[(size_t)g.nfp + j];
+                s[3] += u[2 * (size_t)g.nfp + j];
+                s[4] += 1.0;
+            }
+    for (int c = 0; c < 5; ++c) out[(size_t)k * 5 + c] = s[c];
+}
+
+}  // namespace
+
+int lbf_block_sums(lbf_engine* e, uint32_t block, double* out, size_t n)
+{
+    if (!e || !out || block == 0) return fail(e, LBF_EINVAL, "NULL argument or zero block");
+    if (e->cfg.model != LBF_MODEL_SCSP) return fail(e, LBF_EINVAL, "block sums are single-phase only");
+    const uint32_t bzs = e->D == 2 ? 1u : block;
+    if (e->nx % block || e->ny % block || e->nz % bzs) return fail(e, LBF_EINVAL, "grid is not a multiple of block");
+    const int bx = e->nx / (int)block, by = e->ny / (int)block, bz = e->nz / (int)bzs;
+    const size_t nb = (size_t)bx * by * bz;
+    if (n != nb * 5) return fail(e, LBF_EINVAL, "out must hold 5 doubles per block");
+    if (!e->initialized) return fail(e, LBF_ESTATE, "block sums before initialisation");
+    int rc = setdev(e);
+    if (rc) return rc;
+    double* d = nullptr;
+    LBF_CK(e, cudaMalloc(&d, nb * 5 * sizeof(double)));
+    const Grid g = grid_of(e);
+    if (e->D == 2) {
+        // 2-D: cubes are block x block squares of the single layer.
+        block_sums_kernel<<<blocks_for((uint32_t)nb, 128), 128, 0, e->stream>>>(g, e->rho0, e->u, (int)block, bx, by,
+                                                                                 1, d);
+    } else {
+        block_sums_kernel<<<blocks_for((uint32_t)nb, 128), 128, 0, e->stream>>>(g, e->rho0, e->u, (int)block, bx, by,
+                                                                                 bz, d);
+    }
+    cudaError_t r = cudaGetLastError();
+    if (r == cudaSuccess) r = cudaMemcpyAsync(out, d, nb * 5 * sizeof(double), cudaMemcpyDeviceToHost, e->stream);
+    if (r == cudaSuccess) r = cudaStreamSynchronize(e->stream);
+    cudaFree(d);
+    if (r != cudaSuccess) return fail(e, LBF_ECUDA, std::string("block sums: ") + cudaGetErrorString(r));
+    return LBF_OK;
+}
+
+int lbf_add_density(lbf_engine* e, const float* drho)
+{
+    if (!e || !drho) return fail(e, LBF_EINVAL, "NULL argument");
+    if (e->cfg.model != LBF_MODEL_SCSP) return fail(e, LBF_EINVAL, "density increments are single-phase only");
+    if (!e->initialized) return fail(e, LBF_ESTATE, "density increment before initialisation");
+    int rc = setdev(e);
+    if (rc) return rc;
+    LBF_CK(e, cudaDeviceSynchronize());
+    cudaPointerAttributes pa{};
+    if (cudaPointerGetAttributes(&pa, drho) != cudaSuccess || pa.type != cudaMemoryTypeDevice ||
+        pa.device != e->cfg.device) {
+        cudaGetLastError();
+        return fail(e, LBF_EINVAL, "drho must be device memory of the engine's device");
+    }
+    launch_scsp_add_density(e->D, (int)e->cfg.storage, grid_of(e), drho, e->f[e->cur], e->ex[e->cur],
+                            e->cfg.rho[0], e->stream);
+    LBF_CK(e, cudaGetLastError());
+    return LBF_OK;
+}
+
 int lbf_step(lbf_engine* e, uint32_t nsteps, uint32_t flags)
 {
     if (!e) return fail(e, LBF_EINVAL, "NULL engine");

@@ -38,6 +38,8 @@ struct ColorLaunch {
 void launch_scsp(int dims, int storage, bool mrt, bool pull, int out, const ScspLaunch& a);
 void launch_scsp_init(int dims, int storage, const Grid& g, const Force& F, double rho0,
                       void* f, int8_t* eout, cudaStream_t s);
+void launch_scsp_add_density(int dims, int storage, const Grid& g, const float* drho, void* f, int8_t* eio,
+                             double rho0, cudaStream_t s);
 void launch_scsp_init_eq(int dims, int storage, const Grid& g, const Force& F, double rho0, const float* fields,
                          uint32_t ld, void* f, int8_t* eout, cudaStream_t s);
 void launch_color(int dims, int storage, int collision, bool pull, int out, const ColorLaunch& a);

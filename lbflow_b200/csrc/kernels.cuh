@@ -475,4 +475,32 @@ __global__ void scsp_init_eq(const Grid g, const Force F, double rho0, const flo
     }
 }
 
+// Density increment of a running state: f_q += w_q drho(voxel) at every fluid
+// node, in place on the current populations (shifted storage holds f - w rho0,
+// so the increment is the same).  Momentum is unchanged.
+template <class L, class S>
+__global__ void scsp_add_density(const Grid g, const float* __restrict__ drho, typename S::T* __restrict__ f,
+                                 int8_t* __restrict__ ex, double rho0)
+{
+    using R = typename S::R;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.nf) return;
+    const uint32_t c = g.coord[i];
+    const size_t vox = ((size_t)(c >> 22) * g.ny + ((c >> 11) & 0x7FFu)) * g.nx + (c & 0x7FFu);
+    const R d = R(drho[vox]);
+    R vals[L::Q];
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) {
+        const R wq = R(L::w36f(q)) / R(36);
+        if constexpr (S::blocked) vals[q] = S::load_blk(f + (size_t)q * g.nfp + i, q, (int)ex[i]) + wq * d;
+        else vals[q] = S::load(f + (size_t)q * g.nfp + i, q, R(rho0)) + wq * d;
+    }
+    if constexpr (S::blocked) {
+        S::store_blk(f, g.nfp, i, vals, ex);
+    } else {
+#pragma unroll
+        for (int q = 0; q < L::Q; ++q) S::store(f + (size_t)q * g.nfp + i, vals[q], q, R(rho0));
+    }
+}
+
 }  // namespace lbf

@@ -59,7 +59,28 @@ void init_eq_storage(int storage, const Grid& g, const Force& F, double rho0, co
     default: scsp_init_eq<L, StoreF32<L>><<<blocks, threads, 0, s>>>(g, F, rho0, fields, ld, (float*)f, e); break;
     }
 }
+template <class L>
+void add_density_storage(int storage, const Grid& g, const float* drho, void* f, int8_t* e, double rho0,
+                         cudaStream_t s)
+{
+    const unsigned threads = 256, blocks = blocks_for(g.nf, threads);
+    if (blocks == 0) return;
+    switch (storage) {
+    case LBF_STORE_FP64: scsp_add_density<L, StoreF64><<<blocks, threads, 0, s>>>(g, drho, (double*)f, e, rho0); break;
+    case LBF_STORE_FP16: scsp_add_density<L, StoreF16<L>><<<blocks, threads, 0, s>>>(g, drho, (__half*)f, e, rho0); break;
+    case LBF_STORE_BF16: scsp_add_density<L, StoreBF16<L>><<<blocks, threads, 0, s>>>(g, drho, (__nv_bfloat16*)f, e, rho0); break;
+    case LBF_STORE_BFP16: scsp_add_density<L, StoreBFP16<L>><<<blocks, threads, 0, s>>>(g, drho, (int16_t*)f, e, rho0); break;
+    default: scsp_add_density<L, StoreF32<L>><<<blocks, threads, 0, s>>>(g, drho, (float*)f, e, rho0); break;
+    }
+}
 }  // namespace
+
+void launch_scsp_add_density(int dims, int storage, const Grid& g, const float* drho, void* f, int8_t* e,
+                             double rho0, cudaStream_t s)
+{
+    if (dims == 3) add_density_storage<D3Q19>(storage, g, drho, f, e, rho0, s);
+    else add_density_storage<D2Q9>(storage, g, drho, f, e, rho0, s);
+}
 
 void launch_scsp_init_eq(int dims, int storage, const Grid& g, const Force& F, double rho0, const float* fields,
                          uint32_t ld, void* f, int8_t* e, cudaStream_t s)

@@ -22,7 +22,7 @@ def permeability(engine, tau, g, axis=0):
 
 
 def converge(engine, tau, g, report=1000, tol=1e-6, max_steps=2_000_000, initialized=False,
-             on_report=None, warm=None, patience=5, t0=None):
+             on_report=None, warm=None, patience=5, t0=None, accelerate=None):
     """Step to the reference's convergence criterion; returns a dict with the
     completed steps, wall seconds (device work included), K and the residual history.
 
@@ -33,7 +33,9 @@ def converge(engine, tau, g, report=1000, tol=1e-6, max_steps=2_000_000, initial
     `patience` reports.  Steps
     and seconds count both attempts; `fallback` in the result says whether it
     happened.  t0: perf_counter value the seconds count from (default: the
-    start of this call, after the engine's queued work)."""
+    start of this call, after the engine's queued work).  accelerate:
+    optional callable(t) run after the checks of every report (for example a
+    warmstart.DarcyAccelerator); its work is inside the timed region."""
     engine.synchronize()
     if t0 is None:
         t0 = time.perf_counter()
@@ -69,6 +71,8 @@ def converge(engine, tau, g, report=1000, tol=1e-6, max_steps=2_000_000, initial
             restart()
             continue
         K = permeability(engine, tau, g)
+        if accelerate is not None:
+            accelerate(t)
         if first:
             engine.convergence(first=True)
             first = False

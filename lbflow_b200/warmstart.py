@@ -163,40 +163,34 @@ def _shift(x, s, axis):
     return torch.roll(x, s, dims=axis)
 
 
-def darcy_pressure(q, mob, b, iters=400, rtol=1e-10):
-    """Coarse pressure that makes a block-averaged flux field conservative.
+_AXES = (2, 1, 0)            # x, y, z components live on grid axes W, H, D
 
-    q: (d, h, w, 3) block-mean velocity (x, y, z) of a periodic medium;
-    mob: (d, h, w) block mobility (flux per unit driving force); b: block
-    edge in voxels.  Face fluxes are the means of the two blocks' fluxes and
-    face mobilities the harmonic means of their mobilities (series layers).
-    Solves  sum_faces M_f (phi_nb - phi) / b^2 = div q  with periodic wrap by
-    conjugate gradients preconditioned with the mean-mobility Laplacian
-    (inverted by FFT), so that  q - M grad(phi)  has zero divergence.
-    phi is the pressure over rho0 (p / rho0), zero mean.  FP64 throughout."""
-    q = q.double()
-    mob = mob.double().clamp(min=1e-30)
-    axes = (2, 1, 0)            # x, y, z components live on grid axes W, H, D
-    div = torch.zeros_like(mob)
-    mf = []
-    for c, ax in enumerate(axes):
-        flux = 0.5 * (q[..., c] + _shift(q[..., c], -1, ax))          # face i + 1/2
-        div += (flux - _shift(flux, 1, ax)) / b
+
+def _face_mobility(mob):
+    """Harmonic-mean mobility on the + faces of each block along x, y, z
+    (series layers)."""
+    out = []
+    for ax in _AXES:
         nb = _shift(mob, -1, ax)
-        mf.append(2.0 * mob * nb / (mob + nb))
+        out.append(2.0 * mob * nb / (mob + nb))
+    return out
 
+
+def _solve_periodic(rhs, mf, b, iters=400, rtol=1e-10):
+    """Solve  sum_faces M_f (phi_nb - phi) / b^2 = rhs  on a periodic block
+    grid by conjugate gradients preconditioned with the mean-mobility
+    Laplacian (inverted by FFT).  Zero-mean phi; FP64."""
     def A(phi):
         out = torch.zeros_like(phi)
-        for c, ax in enumerate(axes):
-            grad = (_shift(phi, -1, ax) - phi) / b                   # at face i + 1/2
-            f = mf[c] * grad
+        for c, ax in enumerate(_AXES):
+            f = mf[c] * (_shift(phi, -1, ax) - phi) / b                 # at face i + 1/2
             out += (f - _shift(f, 1, ax)) / b
         return out
 
-    d, h, w = mob.shape
-    kz = torch.fft.fftfreq(d, dtype=torch.float64, device=mob.device)
-    ky = torch.fft.fftfreq(h, dtype=torch.float64, device=mob.device)
-    kx = torch.fft.fftfreq(w, dtype=torch.float64, device=mob.device)
+    d, h, w = rhs.shape
+    kz = torch.fft.fftfreq(d, dtype=torch.float64, device=rhs.device)
+    ky = torch.fft.fftfreq(h, dtype=torch.float64, device=rhs.device)
+    kx = torch.fft.fftfreq(w, dtype=torch.float64, device=rhs.device)
     lap = sum((2.0 * torch.cos(2 * math.pi * k) - 2.0) / b ** 2 for k in
               (kz[:, None, None], ky[None, :, None], kx[None, None, :]))
     mbar = torch.stack(mf).mean()
@@ -205,15 +199,15 @@ def darcy_pressure(q, mob, b, iters=400, rtol=1e-10):
     def M(r):
         return torch.fft.ifftn(torch.fft.fftn(r) * inv).real
 
-    rhs = div - div.mean()
+    rhs = rhs - rhs.mean()
     phi = torch.zeros_like(rhs)
+    nrm = rhs.norm()
+    if nrm == 0:
+        return phi
     r = rhs.clone()
     z = M(r)
     p = z.clone()
     rz = (r * z).sum()
-    nrm = rhs.norm()
-    if nrm == 0:
-        return phi
     for _ in range(iters):
         Ap = A(p)
         alpha = rz / (p * Ap).sum()
@@ -228,6 +222,34 @@ def darcy_pressure(q, mob, b, iters=400, rtol=1e-10):
     return phi - phi.mean()
 
 
+def darcy_pressure(mob, g, b):
+    """Large-scale pressure of the upscaled (Darcy) problem on b^3 blocks.
+
+    mob: (d, h, w) block mobility M (Darcy flux per unit driving force,
+    isotropic); the block flux F = M_f (g x_hat - grad phi) across every face
+    is conserved:  div(M grad phi) = g dM/dx.  phi is the pressure over rho0
+    (p / rho0), zero mean, FP64.  This is the pressure field that the
+    lattice Boltzmann run otherwise builds up by slow pressure diffusion
+    across the whole domain."""
+    mob = mob.double().clamp(min=1e-30)
+    mf = _face_mobility(mob)
+    rhs = g * (mf[0] - _shift(mf[0], 1, _AXES[0])) / b
+    return _solve_periodic(rhs, mf, b)
+
+
+def darcy_pressure_from_flux(q, mob, b):
+    """Coarse pressure that makes a block-averaged flux field conservative:
+    q (d, h, w, 3) block-mean velocity, face flux = mean of the two blocks;
+    solves div(M grad phi) = div q so that q - M grad(phi) is divergence-free."""
+    q = q.double()
+    mob = mob.double().clamp(min=1e-30)
+    div = torch.zeros_like(mob)
+    for c, ax in enumerate(_AXES):
+        flux = 0.5 * (q[..., c] + _shift(q[..., c], -1, ax))
+        div += (flux - _shift(flux, 1, ax)) / b
+    return _solve_periodic(div, _face_mobility(mob), b)
+
+
 def _upsample_periodic(phi, b):
     """Trilinear interpolation of block-centre values to voxel centres, periodic."""
     x = phi[None, None]
@@ -238,33 +260,44 @@ def _upsample_periodic(phi, b):
     return up[0, 0, b:b + d * b, b:b + h * b, b:b + w * b]
 
 
-def coarse_correction(u, fluid, g, block=8):
-    """Density correction (per voxel) that removes the large-scale mass
-    imbalance of a predicted velocity field u (D, H, W, 3) under force g
-    along +x: block fluxes and mobilities from u, darcy_pressure, interpolated
-    to the voxels and converted to density (rho = 3 p at c_s^2 = 1/3)."""
-    b = block
-    q = _block_mean(u.double(), b)
-    mob = q[..., 0] / g
-    mob = torch.clamp(mob, min=1e-3 * float(mob.clamp(min=0).mean()) + 1e-30)
-    phi = darcy_pressure(q, mob, b)
-    return 3.0 * _upsample_periodic(phi, b) * fluid.double()
+def _pore_block_mean(x, m, b):
+    """Pore-weighted block means of a (D, H, W) field (zero where a block has no pores)."""
+    num = _block_mean((x * m)[..., None], b)[..., 0]
+    den = _block_mean(m[..., None], b)[..., 0]
+    return torch.where(den > 0, num / den.clamp(min=1e-30), torch.zeros_like(num))
 
 
-def predict(net, fluid, tau, g, rho0=1.0, block=8):
+def predict(net, fluid, tau, g, rho0=1.0, block=8, mode='darcy'):
     """Warm-start fields (D, H, W, 4) float32 on the GPU: velocity x, y, z and
-    density for force g along +x and relaxation time tau.  block: edge of
-    the coarse Darcy correction (0 = network only)."""
+    density for force g along +x and relaxation time tau.
+
+    mode 'none':  velocity and density deviation 3 g pi straight from the network.
+    mode 'darcy': the network's pi keeps only its structure below the block
+                  scale; the block-scale pressure comes from darcy_pressure
+                  with block mobilities = block means of the network's k_x / nu.
+    mode 'flux':  the network's density plus the pressure that makes its
+                  block fluxes conservative (darcy_pressure_from_flux)."""
     with torch.no_grad():
         f = features(fluid.unsqueeze(0))
         y = net(f)[0, ..., :4].float() * net.scale
-        m = fluid.float()
+        m = fluid.double()
         nu = (tau - 0.5) / 3.0
         out = torch.empty(*fluid.shape, 4, dtype=torch.float32, device=fluid.device)
-        out[..., :3] = y[..., :3] * (g / nu) * m[..., None]
-        drho = 3.0 * g * y[..., 3].double() * m
-        if block:
-            drho = drho + coarse_correction(out[..., :3], fluid, g, block)
+        out[..., :3] = y[..., :3] * (g / nu) * m[..., None].float()
+        pi = y[..., 3].double() * m
+        if mode == 'darcy' and block:
+            pi = pi - _upsample_periodic(_pore_block_mean(pi, m, block), block) * m
+            mob = _block_mean(out[..., :1].double(), block)[..., 0] / g
+            mob = torch.clamp(mob, min=1e-3 * float(mob.clamp(min=0).mean()) + 1e-30)
+            phi = darcy_pressure(mob, g, block)
+            drho = 3.0 * g * pi + 3.0 * rho0 * _upsample_periodic(phi, block) * m
+        elif mode == 'flux' and block:
+            q = _block_mean(out[..., :3].double(), block)
+            mob = torch.clamp(q[..., 0] / g, min=1e-3 * float(q[..., 0].clamp(min=0).mean() / g) + 1e-30)
+            phi = darcy_pressure_from_flux(q, mob, block)
+            drho = 3.0 * g * pi + 3.0 * rho0 * _upsample_periodic(phi, block) * m
+        else:
+            drho = 3.0 * g * pi
         # Zero-mean density deviation over the pores (mass of the rest state).
         drho = drho - drho.sum() / m.sum().clamp(min=1.0) * m
         out[..., 3] = (rho0 + drho).float()
@@ -272,12 +305,65 @@ def predict(net, fluid, tau, g, rho0=1.0, block=8):
         return out.contiguous()
 
 
-def warm_start(engine, net, fluid, tau, g, rho0=1.0, block=8):
+def warm_start(engine, net, fluid, tau, g, rho0=1.0, block=8, mode='darcy'):
     """Initialise `engine` from the network's prediction; returns the fields."""
-    fields = predict(net, fluid, tau, g, rho0, block)
+    fields = predict(net, fluid, tau, g, rho0, block, mode)
     torch.cuda.current_stream(fluid.device).synchronize()
-    engine.initialize_equilibrium(fields.data_ptr(), 4)
+    engine.initialize_equilibrium(fields)
     return fields
+
+
+class DarcyAccelerator:
+    """Coarse pressure correction of a running single-phase engine.
+
+    After the fast viscous transient the flow in each b^3 block is the local
+    Darcy response  q = M (g x_hat - grad phi)  to the current pressure phi,
+    while phi itself still creeps towards steady state by pressure diffusion
+    across the domain -- the slowest mode of the run.  At each report step in
+    `at` the accelerator reads the block sums (lbf_block_sums), estimates M
+    per block from q and the block pressure gradient (least squares over the
+    three components), solves the upscaled problem for the steady block
+    pressure (darcy_pressure) and adds the difference as a density change at
+    unchanged momentum (lbf_add_density).  Mass is conserved and the
+    lattice Boltzmann fixed point is unchanged, so the converged answer is
+    the solver's own; only the slow mode is shortened.  3-D, force along +x."""
+
+    def __init__(self, engine, fluid, g, rho0=1.0, block=8, at=(1000,)):
+        self.engine, self.g, self.rho0, self.b = engine, g, rho0, block
+        self.fluid = fluid.double()
+        self.at = set(int(t) for t in at)
+        self.applied = []
+
+    def __call__(self, t):
+        if t not in self.at:
+            return False
+        self.apply()
+        self.applied.append(t)
+        return True
+
+    def apply(self):
+        b, g, rho0 = self.b, self.g, self.rho0
+        dev = self.fluid.device
+        s = torch.from_numpy(self.engine.block_sums(b)).to(dev)
+        cnt = s[..., 4]
+        rho_b = torch.where(cnt > 0, s[..., 0] / cnt.clamp(min=1.0), torch.full_like(cnt, rho0))
+        q = s[..., 1:4] / float(b ** 3)
+        phi = (rho_b - rho0) / (3.0 * rho0)
+        drive = []
+        for c, ax in enumerate(_AXES):
+            grad = (_shift(phi, -1, ax) - _shift(phi, 1, ax)) / (2.0 * b)
+            drive.append((g if c == 0 else 0.0) - grad)
+        num = sum(q[..., c] * drive[c] for c in range(3))
+        den = sum(d * d for d in drive)
+        mob = torch.where(den > 0, num / den.clamp(min=1e-300), torch.zeros_like(num))
+        mob = torch.clamp(mob, min=1e-3 * float(mob.clamp(min=0).mean()) + 1e-30)
+        target = darcy_pressure(mob, g, b)
+        porous = cnt > 0
+        cur = phi - (phi * porous).sum() / porous.sum().clamp(min=1)
+        dphi = (target - cur) * porous
+        drho = 3.0 * rho0 * _upsample_periodic(dphi, b) * self.fluid
+        drho = drho - drho.sum() / self.fluid.sum().clamp(min=1.0) * self.fluid
+        self.engine.add_density(drho.float().contiguous())
 
 
 def save(net, path, meta=None):

@@ -147,28 +147,25 @@ def test_darcy_pressure_layered_medium():
     D, H, W = 8, 8, 128
     x = (torch.arange(W, dtype=torch.float64) + 0.5) / W
     M = 1.0 + 0.6 * torch.sin(2 * math.pi * x)                     # voxel mobility along x
-    u = torch.zeros(D, H, W, 3, dtype=torch.float64)
-    u[..., 0] = (M * g).expand(D, H, W)                            # local response, no pressure
-    q = ws._block_mean(u, b)
-    mob = q[..., 0] / g
-    phi = ws.darcy_pressure(q, mob, b)
-    # Corrected block-face flux along x is uniform (= divergence-free in 1D).
+    mob = ws._block_mean(M.expand(D, H, W)[..., None], b)[..., 0]
+    phi = ws.darcy_pressure(mob, g, b)
     mf = 2 * mob * torch.roll(mob, -1, 2) / (mob + torch.roll(mob, -1, 2))
-    face = 0.5 * (q[..., 0] + torch.roll(q[..., 0], -1, 2)) - mf * (torch.roll(phi, -1, 2) - phi) / b
+    face = mf * (g - (torch.roll(phi, -1, 2) - phi) / b)            # x flux through each + face
     assert float(face.std() / face.mean()) < 1e-8
-    # Its value approaches the harmonic mean mobility times g.
     qh = g / float((1.0 / M).mean())
     assert abs(float(face.mean()) - qh) < 0.02 * qh
-    # Pressure: phi(x) = integral of (g - q/M); compare the profile at block centres.
     xc = (torch.arange(W // b, dtype=torch.float64) + 0.5) * b
-    dphi = g - qh / M
-    prof = torch.cumsum(dphi, 0)
-    prof = prof - prof.mean()
+    prof = torch.cumsum(g - qh / M, 0)
     ref = prof[(xc - 0.5).long()]
     ref = ref - ref.mean()
     got = phi[0, 0]
     assert float((got - ref).norm() / ref.norm()) < 0.05
     assert torch.allclose(phi[1, 1], phi[0, 0])                    # uniform across y, z
+    # The flux form gives the same pressure from the local response M g.
+    q = torch.zeros(D // b, H // b, W // b, 3, dtype=torch.float64)
+    q[..., 0] = mob * g
+    phi2 = ws.darcy_pressure_from_flux(q, mob, b)
+    assert float((phi2 - phi).norm() / phi.norm()) < 0.05
 
 
 def test_darcy_pressure_removes_divergence_3d():
@@ -177,7 +174,7 @@ def test_darcy_pressure_removes_divergence_3d():
     q = torch.rand(6, 8, 10, 3, generator=gen, dtype=torch.float64) * 1e-5
     mob = 0.5 + torch.rand(6, 8, 10, generator=gen, dtype=torch.float64)
     b = 8
-    phi = ws.darcy_pressure(q, mob, b)
+    phi = ws.darcy_pressure_from_flux(q, mob, b)
     div = torch.zeros_like(mob)
     for c, ax in enumerate((2, 1, 0)):
         nb = torch.roll(mob, -1, ax)

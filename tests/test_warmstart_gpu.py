@@ -196,7 +196,7 @@ def test_initialize_equilibrium_reproduces_fields(storage, tol):
     dev = torch.from_numpy(f).cuda()
     torch.cuda.synchronize()
     with Engine(geom, LABELS, collision='MRT', tau=(1.0,), storage=storage) as e:
-        e.initialize_equilibrium(dev.data_ptr(), 4)
+        e.initialize_equilibrium(dev)
         e.check()
         rho, _, u = e.macros()
     fl = fluid
@@ -217,11 +217,11 @@ def test_warm_start_from_converged_field_converges_at_once():
         rho, _, u = e.macros()
     assert cold['converged']
     fields = np.concatenate([np.moveaxis(u, 0, -1), rho[..., None]], -1).astype(np.float32)
-    dev = torch.from_numpy(fields).cuda()
+    dev = torch.from_numpy(fields).cuda().contiguous()
     torch.cuda.synchronize()
     with Engine(geom, LABELS, collision='MRT', tau=(0.8,)) as e:
         warm = converge(e, 0.8, 1e-5, report=500, tol=1e-8,
-                        warm=lambda: e.initialize_equilibrium(dev.data_ptr(), 4))
+                        warm=lambda: e.initialize_equilibrium(dev))
     print(f"cold {cold['steps']} steps, warm {warm['steps']} steps")
     assert warm['converged'] and not warm['fallback']
     assert warm['steps'] <= cold['steps'] / 3
@@ -249,3 +249,44 @@ def test_trained_operator_reaches_band_sooner():
     tw = time_to_band(runs['warm']['history'], K)
     print(f'steps to the 1e-3 band: cold {tc[0]}, warm {tw[0]}')
     assert tw[0] < tc[0]
+
+
+def test_block_sums_match_dense_macros():
+    from lbflow_b200 import Engine
+    from lbflow_b200.geometry import porous_medium
+    fluid = porous_medium((16, 24, 32), sigma=2.0, porosity=0.3, seed=4)
+    geom = np.where(fluid, 75, 255).astype(np.uint8)
+    with Engine(geom, LABELS, collision='MRT', tau=(0.9,)) as e:
+        e.initialize()
+        e.step(200, macros=True)
+        rho, _, u = e.macros()
+        s = e.block_sums(8)
+    assert s.shape == (2, 3, 4, 5)
+    blk = lambda a: a.reshape(2, 8, 3, 8, 4, 8).sum(axis=(1, 3, 5))
+    assert np.array_equal(s[..., 4], blk(fluid.astype(float)))
+    assert np.allclose(s[..., 0], blk(rho), rtol=1e-13, atol=0)
+    for c in range(3):
+        assert np.allclose(s[..., 1 + c], blk(u[c]), rtol=1e-11, atol=1e-20)
+
+
+@pytest.mark.parametrize('storage,tol', [('fp64', 1e-15), ('fp32', 1e-9), ('bfp16', 1e-7)])
+def test_add_density_shifts_populations(storage, tol):
+    from lbflow_b200 import Engine
+    from lbflow_b200.geometry import porous_medium
+    fluid = porous_medium((16, 16, 24), sigma=2.0, porosity=0.35, seed=6)
+    geom = np.where(fluid, 75, 255).astype(np.uint8)
+    rng = np.random.default_rng(3)
+    drho = (rng.standard_normal(fluid.shape) * 1e-4).astype(np.float32)
+    w = np.array([12] + [2] * 6 + [1] * 12) / 36.0
+    with Engine(geom, LABELS, collision='MRT', tau=(1.0,), storage=storage) as e:
+        e.initialize()
+        e.step(30)
+        f0 = e.populations()
+        d = torch.from_numpy(drho).cuda().contiguous()
+        torch.cuda.synchronize()
+        e.add_density(d)
+        f1 = e.populations()
+        e.check()
+    expect = f0 + w[None, :, None, None, None] * np.where(fluid, drho, 0.0)[None, None]
+    assert np.max(np.abs(f1[:, :, fluid] - expect[:, :, fluid])) <= tol + 1e-6 * tol
+    assert np.all(f1[:, :, ~fluid] == 0)
