@@ -131,7 +131,9 @@ int lbf_initialize_equilibrium(lbf_engine *e, const float *fields, uint32_t ld, 
  * be multiples of block (nz = 1 in 2-D is taken as one layer); out: host,
  * n = (nx/block)(ny/block)(nz/block) * 5 doubles, cube (bz, by, bx) at
  * ((bz * NBy + by) * NBx + bx) * 5: { sum rho, sum u_x, sum u_y, sum u_z,
- * fluid voxels } over its fluid voxels, summed in voxel order. */
+ * fluid voxels } over its fluid voxels, summed in voxel order.  out may be
+ * host memory or device memory of the engine's device (filled without a
+ * host round trip); the call returns when the sums are written. */
 int lbf_block_sums(lbf_engine *e, uint32_t block, double *out, size_t n);
 
 /* Adds w_q * drho(voxel) to every population of every fluid node of the
@@ -140,6 +142,19 @@ int lbf_block_sums(lbf_engine *e, uint32_t block, double *out, size_t n);
  * (z, y, x) order; solid voxels are ignored.  Waits for all queued device
  * work first, like lbf_initialize_equilibrium. */
 int lbf_add_density(lbf_engine *e, const float *drho);
+
+/* Block-scale Darcy pressure of a periodic porous medium (the solve of the
+ * convergence accelerator; LBFlow has no counterpart): mob = DEVICE
+ * double[nz][ny][nx], the Darcy mobility (flux per unit driving force) of
+ * each block of edge h voxels; g: body force along +x.  Writes the
+ * zero-mean pressure over rho0, phi (DEVICE double[nz][ny][nx]), whose block
+ * fluxes M_f (g [x face] - grad phi) across block faces (M_f: geometric mean
+ * of the two blocks) are conserved.  Multigrid-preconditioned conjugate
+ * gradients stopped at relative residual rtol or max_iter iterations
+ * (reported in *iterations).  The extents must halve down to a grid of at
+ * most 1024 cells.  Runs on `stream`; returns after the result is written. */
+int lbf_darcy_pressure(const double *mob, uint32_t nz, uint32_t ny, uint32_t nx, double h, double g,
+                       double rtol, uint32_t max_iter, double *phi, uint32_t *iterations, void *stream);
 
 /* nsteps steps of the Run loop body: streaming, bounce-back, calcMacroVar,
  * bodyForce, collision (scsp.cpp:75-104; colorfluid.cpp:142-198).  flags

@@ -80,6 +80,8 @@ def library():
             'lbf_initialize_equilibrium': (I, [P, P, U32, U32]),
             'lbf_block_sums': (I, [P, U32, D, ctypes.c_size_t]),
             'lbf_add_density': (I, [P, P]),
+            'lbf_darcy_pressure': (I, [P, U32, U32, U32, ctypes.c_double, ctypes.c_double, ctypes.c_double, U32, P,
+                                       ctypes.POINTER(U32), P]),
             'lbf_step': (I, [P, U32, U32]),
             'lbf_get_populations': (I, [P, D, ctypes.c_size_t]),
             'lbf_set_populations': (I, [P, D, ctypes.c_size_t]),
@@ -189,15 +191,23 @@ class Engine:
     def initialize(self):
         self._ck(self._lib.lbf_initialize(self._h))
 
-    def block_sums(self, block):
-        """Per-cube sums of the last written fields: array (NBz, NBy, NBx, 5) of
-        (sum rho, sum u_x, sum u_y, sum u_z, fluid voxels)."""
+    def block_sums(self, block, out=None):
+        """Per-cube sums of the last written fields, (NBz, NBy, NBx, 5) of
+        (sum rho, sum u_x, sum u_y, sum u_z, fluid voxels): a numpy array, or
+        written into `out` (a contiguous float64 CUDA tensor of that shape)."""
         nz, ny, nx = (1,) + tuple(self.shape) if len(self.shape) == 2 else tuple(self.shape)
         bz = 1 if len(self.shape) == 2 else block
         shp = (nz // bz, ny // block, nx // block, 5)
-        out = np.zeros(shp)
-        self._ck(self._lib.lbf_block_sums(self._h, int(block), _dptr(out), out.size))
-        return out
+        if out is not None:
+            if (tuple(out.shape) != shp or str(out.dtype) != 'torch.float64' or not out.is_cuda
+                    or not out.is_contiguous()):
+                raise ValueError(f'out must be a contiguous float64 CUDA tensor of shape {shp}')
+            ptr = ctypes.cast(ctypes.c_void_p(out.data_ptr()), ctypes.POINTER(ctypes.c_double))
+            self._ck(self._lib.lbf_block_sums(self._h, int(block), ptr, out.numel()))
+            return out
+        res = np.zeros(shp)
+        self._ck(self._lib.lbf_block_sums(self._h, int(block), _dptr(res), res.size))
+        return res
 
     def add_density(self, drho):
         """Add w_q * drho to the current populations (contiguous float32 CUDA

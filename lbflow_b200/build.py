@@ -26,7 +26,7 @@ NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 NVFLAGS = ['-std=c++17', '-O3', '-lineinfo', '--expt-relaxed-constexpr', '-Xcompiler', '-fPIC',
            '-Xcompiler', '-O3'] + ARCH
-CUDA_UNITS = ['engine.cu', 'scsp_launch.cu', 'color_launch.cu', 'noalloc.cu', 'batch.cu', 'conv.cu']
+CUDA_UNITS = ['engine.cu', 'scsp_launch.cu', 'color_launch.cu', 'noalloc.cu', 'batch.cu', 'conv.cu', 'darcy.cu']
 HOST_UNITS = ['main.cpp', 'prm.cpp', 'io.cpp', 'simulation.cpp']
 LIBNAME = 'liblbflow_b200.so'
 

@@ -714,8 +714,13 @@ int lbf_block_sums(lbf_engine* e, uint32_t block, double* out, size_t n)
     if (!e->initialized) return fail(e, LBF_ESTATE, "block sums before initialisation");
     int rc = setdev(e);
     if (rc) return rc;
-    double* d = nullptr;
-    LBF_CK(e, cudaMalloc(&d, nb * 5 * sizeof(double)));
+    // out may be device memory of the engine's device (written in place) or host memory.
+    cudaPointerAttributes pa{};
+    const bool on_device = cudaPointerGetAttributes(&pa, out) == cudaSuccess && pa.type == cudaMemoryTypeDevice;
+    cudaGetLastError();
+    if (on_device && pa.device != e->cfg.device) return fail(e, LBF_EINVAL, "out is device memory of another device");
+    double* d = on_device ? out : nullptr;
+    if (!on_device) LBF_CK(e, cudaMalloc(&d, nb * 5 * sizeof(double)));
     const Grid g = grid_of(e);
     if (e->D == 2) {
         // 2-D: cubes are block x block squares of the single layer.
@@ -726,9 +731,10 @@ int lbf_block_sums(lbf_engine* e, uint32_t block, double* out, size_t n)
                                                                                  bz, d);
     }
     cudaError_t r = cudaGetLastError();
-    if (r == cudaSuccess) r = cudaMemcpyAsync(out, d, nb * 5 * sizeof(double), cudaMemcpyDeviceToHost, e->stream);
+    if (!on_device && r == cudaSuccess)
+        r = cudaMemcpyAsync(out, d, nb * 5 * sizeof(double), cudaMemcpyDeviceToHost, e->stream);
     if (r == cudaSuccess) r = cudaStreamSynchronize(e->stream);
-    cudaFree(d);
+    if (!on_device) cudaFree(d);
     if (r != cudaSuccess) return fail(e, LBF_ECUDA, std::string("block sums: ") + cudaGetErrorString(r));
     return LBF_OK;
 }

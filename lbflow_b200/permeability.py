@@ -71,8 +71,8 @@ def converge(engine, tau, g, report=1000, tol=1e-6, max_steps=2_000_000, initial
             restart()
             continue
         K = permeability(engine, tau, g)
-        if accelerate is not None:
-            accelerate(t)
+        if accelerate is not None and accelerate(t):
+            best, since_best = math.inf, 0       # a correction restarts the stall watch
         if first:
             engine.convergence(first=True)
             first = False

@@ -166,53 +166,145 @@ def _shift(x, s, axis):
 _AXES = (2, 1, 0)            # x, y, z components live on grid axes W, H, D
 
 
-def _face_mobility(mob):
-    """Harmonic-mean mobility on the + faces of each block along x, y, z
-    (series layers)."""
+def _face_mobility(mob, face='geometric'):
+    """Mobility on the + faces of each block along x, y, z: the geometric mean
+    of the two blocks (the effective-medium value for random media, between
+    the series (harmonic) and parallel (arithmetic) bounds), or either bound."""
     out = []
     for ax in _AXES:
         nb = _shift(mob, -1, ax)
-        out.append(2.0 * mob * nb / (mob + nb))
+        if face == 'geometric':
+            out.append(torch.sqrt(mob * nb))
+        elif face == 'arithmetic':
+            out.append(0.5 * (mob + nb))
+        else:
+            out.append(2.0 * mob * nb / (mob + nb))
     return out
 
 
-def _solve_periodic(rhs, mf, b, iters=400, rtol=1e-10):
+def _apply(phi, mf, h):
+    """Variable-coefficient periodic Laplacian sum_faces M_f (phi_nb - phi) / h^2."""
+    out = torch.zeros_like(phi)
+    for c, ax in enumerate(_AXES):
+        f = mf[c] * (_shift(phi, -1, ax) - phi)                     # at face i + 1/2
+        out += f - _shift(f, 1, ax)
+    return out / (h * h)
+
+
+def _diag(mf, h):
+    d = torch.zeros_like(mf[0])
+    for c, ax in enumerate(_AXES):
+        d -= mf[c] + _shift(mf[c], 1, ax)
+    return d / (h * h)
+
+
+def _coarsen_faces(mf):
+    """Face mobilities of the 2x-coarser grid: the mean of the four fine faces
+    on each coarse interface (flux-consistent for a linear pressure)."""
+    out = []
+    for c, ax in enumerate(_AXES):
+        m = mf[c]
+        # The fine faces on coarse interfaces have an odd index along ax.
+        m = torch.index_select(m, ax, torch.arange(1, m.shape[ax], 2, device=m.device))
+        for o in _AXES:
+            if o == ax:
+                continue
+            shp = list(m.shape)
+            shp[o:o + 1] = [shp[o] // 2, 2]
+            m = m.reshape(shp).mean(dim=o + 1)
+        out.append(m)
+    return out
+
+
+def _prolong(e):
+    """Periodic trilinear prolongation of cell-centred values to the 2x-finer
+    grid: fine cell 2i takes 3/4 e_i + 1/4 e_(i-1), fine cell 2i+1 takes
+    3/4 e_i + 1/4 e_(i+1), along each axis."""
+    for ax in (0, 1, 2):
+        lo = 0.75 * e + 0.25 * _shift(e, 1, ax)
+        hi = 0.75 * e + 0.25 * _shift(e, -1, ax)
+        e = torch.stack([lo, hi], dim=ax + 1).flatten(ax, ax + 1)
+    return e
+
+
+def _restrict(r):
+    """Adjoint of _prolong divided by 8: weights 1/8, 3/8, 3/8, 1/8 of the fine
+    cells 2i-1 .. 2i+2 along each axis (so the V-cycle stays symmetric)."""
+    for ax in (0, 1, 2):
+        n = r.shape[ax] // 2
+        ev = torch.index_select(r, ax, torch.arange(0, 2 * n, 2, device=r.device))
+        od = torch.index_select(r, ax, torch.arange(1, 2 * n, 2, device=r.device))
+        r = 0.375 * (ev + od) + 0.125 * (_shift(od, 1, ax) + _shift(ev, -1, ax))
+    return r
+
+
+class _Multigrid:
+    """Symmetric V-cycle for the periodic variable-coefficient Laplacian
+    (damped Jacobi, trilinear prolongation, its adjoint as restriction, face
+    mobilities averaged over coarse interfaces, a dense pseudo-inverse on the
+    coarsest grid), the conjugate-gradient preconditioner.  FP32."""
+
+    def __init__(self, mf, h, nu=2, omega=0.7, max_coarse=512):
+        mf = [m.float() for m in mf]
+        self.levels = []
+        while True:
+            self.levels.append((mf, h, _diag(mf, h)))
+            shape = mf[0].shape
+            if mf[0].numel() <= max_coarse or any(n % 2 for n in shape):
+                break
+            mf, h = _coarsen_faces(mf), 2 * h
+        cmf, ch, _ = self.levels[-1]
+        shape = cmf[0].shape
+        n = cmf[0].numel()
+        eye = torch.eye(n, dtype=torch.float64, device=cmf[0].device).reshape(n, *shape)
+        A = torch.stack([_apply(eye[k], [m.double() for m in cmf], ch).reshape(-1) for k in range(n)], dim=1)
+        self.coarse_inv = torch.linalg.pinv(A).float()
+        self.coarse_shape = shape
+        self.nu, self.omega = nu, omega
+
+    def _smooth(self, x, r, lvl, sweeps):
+        mf, h, dg = self.levels[lvl]
+        for _ in range(sweeps):
+            x = x + self.omega * (r - _apply(x, mf, h)) / dg
+        return x
+
+    def _cycle(self, r, lvl):
+        mf, h, _ = self.levels[lvl]
+        if lvl == len(self.levels) - 1:
+            x = (self.coarse_inv @ (r - r.mean()).reshape(-1)).reshape(self.coarse_shape)
+            return x - x.mean()
+        x = self._smooth(torch.zeros_like(r), r, lvl, self.nu)
+        rc = _restrict(r - _apply(x, mf, h))
+        x = x + _prolong(self._cycle(rc - rc.mean(), lvl + 1))
+        return self._smooth(x, r, lvl, self.nu)
+
+    def __call__(self, r):
+        return self._cycle(r.float(), 0).double()
+
+
+def _solve_periodic(rhs, mf, b, iters=200, rtol=1e-8):
     """Solve  sum_faces M_f (phi_nb - phi) / b^2 = rhs  on a periodic block
-    grid by conjugate gradients preconditioned with the mean-mobility
-    Laplacian (inverted by FFT).  Zero-mean phi; FP64."""
-    def A(phi):
-        out = torch.zeros_like(phi)
-        for c, ax in enumerate(_AXES):
-            f = mf[c] * (_shift(phi, -1, ax) - phi) / b                 # at face i + 1/2
-            out += (f - _shift(f, 1, ax)) / b
-        return out
-
-    d, h, w = rhs.shape
-    kz = torch.fft.fftfreq(d, dtype=torch.float64, device=rhs.device)
-    ky = torch.fft.fftfreq(h, dtype=torch.float64, device=rhs.device)
-    kx = torch.fft.fftfreq(w, dtype=torch.float64, device=rhs.device)
-    lap = sum((2.0 * torch.cos(2 * math.pi * k) - 2.0) / b ** 2 for k in
-              (kz[:, None, None], ky[None, :, None], kx[None, None, :]))
-    mbar = torch.stack(mf).mean()
-    inv = torch.where(lap.abs() > 0, 1.0 / (mbar * lap), torch.zeros_like(lap))
-
-    def M(r):
-        return torch.fft.ifftn(torch.fft.fftn(r) * inv).real
-
+    grid by conjugate gradients (FP64) preconditioned with a multigrid
+    V-cycle, robust to the orders-of-magnitude mobility contrast of a porous
+    medium.  Zero-mean phi.  The iteration count is left in
+    _solve_periodic.iterations."""
     rhs = rhs - rhs.mean()
     phi = torch.zeros_like(rhs)
     nrm = rhs.norm()
+    _solve_periodic.iterations = 0
     if nrm == 0:
         return phi
+    M = _Multigrid(mf, float(b))
     r = rhs.clone()
     z = M(r)
     p = z.clone()
     rz = (r * z).sum()
-    for _ in range(iters):
-        Ap = A(p)
+    for it in range(iters):
+        Ap = _apply(p, mf, float(b))
         alpha = rz / (p * Ap).sum()
         phi = phi + alpha * p
         r = r - alpha * Ap
+        _solve_periodic.iterations = it + 1
         if r.norm() <= rtol * nrm:
             break
         z = M(r)
@@ -222,7 +314,7 @@ def _solve_periodic(rhs, mf, b, iters=400, rtol=1e-10):
     return phi - phi.mean()
 
 
-def darcy_pressure(mob, g, b):
+def darcy_pressure(mob, g, b, rtol=1e-8, face='geometric'):
     """Large-scale pressure of the upscaled (Darcy) problem on b^3 blocks.
 
     mob: (d, h, w) block mobility M (Darcy flux per unit driving force,
@@ -230,14 +322,34 @@ def darcy_pressure(mob, g, b):
     is conserved:  div(M grad phi) = g dM/dx.  phi is the pressure over rho0
     (p / rho0), zero mean, FP64.  This is the pressure field that the
     lattice Boltzmann run otherwise builds up by slow pressure diffusion
-    across the whole domain."""
+    across the whole domain.  The torch implementation here is the reference
+    of the library's CUDA solve (darcy_pressure_device)."""
     mob = mob.double().clamp(min=1e-30)
-    mf = _face_mobility(mob)
+    mf = _face_mobility(mob, face)
     rhs = g * (mf[0] - _shift(mf[0], 1, _AXES[0])) / b
-    return _solve_periodic(rhs, mf, b)
+    return _solve_periodic(rhs, mf, b, rtol=rtol)
 
 
-def darcy_pressure_from_flux(q, mob, b):
+def darcy_pressure_device(mob, g, b, rtol=1e-3, max_iter=200):
+    """darcy_pressure (geometric face means) by the library's CUDA solver
+    (lbf_darcy_pressure: multigrid-preconditioned conjugate gradients) on a
+    CUDA tensor of block mobilities; returns (phi, iterations)."""
+    import ctypes
+    from . import LbfError, library
+    lib = library()
+    mob = mob.double().contiguous()
+    phi = torch.empty_like(mob)
+    it = ctypes.c_uint32(0)
+    nz, ny, nx = mob.shape
+    rc = lib.lbf_darcy_pressure(ctypes.c_void_p(mob.data_ptr()), nz, ny, nx, float(b), float(g), float(rtol),
+                                int(max_iter), ctypes.c_void_p(phi.data_ptr()), ctypes.byref(it),
+                                ctypes.c_void_p(torch.cuda.current_stream(mob.device).cuda_stream))
+    if rc != 0:
+        raise LbfError(rc, lib.lbf_last_error(None).decode())
+    return phi, int(it.value)
+
+
+def darcy_pressure_from_flux(q, mob, b, face='geometric'):
     """Coarse pressure that makes a block-averaged flux field conservative:
     q (d, h, w, 3) block-mean velocity, face flux = mean of the two blocks;
     solves div(M grad phi) = div q so that q - M grad(phi) is divergence-free."""
@@ -247,7 +359,7 @@ def darcy_pressure_from_flux(q, mob, b):
     for c, ax in enumerate(_AXES):
         flux = 0.5 * (q[..., c] + _shift(q[..., c], -1, ax))
         div += (flux - _shift(flux, 1, ax)) / b
-    return _solve_periodic(div, _face_mobility(mob), b)
+    return _solve_periodic(div, _face_mobility(mob, face), b)
 
 
 def _upsample_periodic(phi, b):
@@ -267,7 +379,19 @@ def _pore_block_mean(x, m, b):
     return torch.where(den > 0, num / den.clamp(min=1e-30), torch.zeros_like(num))
 
 
-def predict(net, fluid, tau, g, rho0=1.0, block=8, mode='darcy'):
+def _smooth121(x, m):
+    """Mask-normalised [1, 2, 1] / 4 filter along each axis (periodic) of a
+    (D, H, W) field over the pores m: removes the grid-scale (Nyquist)
+    component of a predicted field, which the lattice Boltzmann run would
+    otherwise carry as a slowly decaying staggered mode."""
+    num, den = x * m, m.clone()
+    for ax in (0, 1, 2):
+        num = 0.25 * (_shift(num, 1, ax) + 2.0 * num + _shift(num, -1, ax))
+        den = 0.25 * (_shift(den, 1, ax) + 2.0 * den + _shift(den, -1, ax))
+    return torch.where(den > 0, num / den.clamp(min=1e-30), torch.zeros_like(num)) * m
+
+
+def predict(net, fluid, tau, g, rho0=1.0, block=8, mode='darcy', velocity=True, smooth=True):
     """Warm-start fields (D, H, W, 4) float32 on the GPU: velocity x, y, z and
     density for force g along +x and relaxation time tau.
 
@@ -276,20 +400,26 @@ def predict(net, fluid, tau, g, rho0=1.0, block=8, mode='darcy'):
                   scale; the block-scale pressure comes from darcy_pressure
                   with block mobilities = block means of the network's k_x / nu.
     mode 'flux':  the network's density plus the pressure that makes its
-                  block fluxes conservative (darcy_pressure_from_flux)."""
+                  block fluxes conservative (darcy_pressure_from_flux).
+    velocity=False starts from rest with the predicted density only (the
+    velocity relaxes to the pressure within the fast viscous transient).
+    smooth: [1, 2, 1] filter of the predicted fields (_smooth121)."""
     with torch.no_grad():
         f = features(fluid.unsqueeze(0))
         y = net(f)[0, ..., :4].float() * net.scale
         m = fluid.double()
         nu = (tau - 0.5) / 3.0
+        yd = y.double()
+        if smooth:
+            yd = torch.stack([_smooth121(yd[..., c], m) for c in range(4)], dim=-1)
         out = torch.empty(*fluid.shape, 4, dtype=torch.float32, device=fluid.device)
-        out[..., :3] = y[..., :3] * (g / nu) * m[..., None].float()
-        pi = y[..., 3].double() * m
+        out[..., :3] = (yd[..., :3] * (g / nu) * m[..., None]).float()
+        pi = yd[..., 3] * m
         if mode == 'darcy' and block:
             pi = pi - _upsample_periodic(_pore_block_mean(pi, m, block), block) * m
             mob = _block_mean(out[..., :1].double(), block)[..., 0] / g
             mob = torch.clamp(mob, min=1e-3 * float(mob.clamp(min=0).mean()) + 1e-30)
-            phi = darcy_pressure(mob, g, block)
+            phi = darcy_pressure(mob, g, block, rtol=1e-4)
             drho = 3.0 * g * pi + 3.0 * rho0 * _upsample_periodic(phi, block) * m
         elif mode == 'flux' and block:
             q = _block_mean(out[..., :3].double(), block)
@@ -298,6 +428,8 @@ def predict(net, fluid, tau, g, rho0=1.0, block=8, mode='darcy'):
             drho = 3.0 * g * pi + 3.0 * rho0 * _upsample_periodic(phi, block) * m
         else:
             drho = 3.0 * g * pi
+        if not velocity:
+            out[..., :3] = 0.0
         # Zero-mean density deviation over the pores (mass of the rest state).
         drho = drho - drho.sum() / m.sum().clamp(min=1.0) * m
         out[..., 3] = (rho0 + drho).float()
@@ -305,46 +437,64 @@ def predict(net, fluid, tau, g, rho0=1.0, block=8, mode='darcy'):
         return out.contiguous()
 
 
-def warm_start(engine, net, fluid, tau, g, rho0=1.0, block=8, mode='darcy'):
+def warm_start(engine, net, fluid, tau, g, rho0=1.0, block=8, mode='darcy', velocity=True, smooth=True):
     """Initialise `engine` from the network's prediction; returns the fields."""
-    fields = predict(net, fluid, tau, g, rho0, block, mode)
+    fields = predict(net, fluid, tau, g, rho0, block, mode, velocity, smooth)
     torch.cuda.current_stream(fluid.device).synchronize()
     engine.initialize_equilibrium(fields)
     return fields
 
 
 class DarcyAccelerator:
-    """Coarse pressure correction of a running single-phase engine.
+    """Block-scale pressure correction of a running single-phase engine.
 
     After the fast viscous transient the flow in each b^3 block is the local
     Darcy response  q = M (g x_hat - grad phi)  to the current pressure phi,
     while phi itself still creeps towards steady state by pressure diffusion
-    across the domain -- the slowest mode of the run.  At each report step in
-    `at` the accelerator reads the block sums (lbf_block_sums), estimates M
-    per block from q and the block pressure gradient (least squares over the
-    three components), solves the upscaled problem for the steady block
-    pressure (darcy_pressure) and adds the difference as a density change at
-    unchanged momentum (lbf_add_density).  Mass is conserved and the
-    lattice Boltzmann fixed point is unchanged, so the converged answer is
-    the solver's own; only the slow mode is shortened.  3-D, force along +x."""
+    across the domain -- the slowest modes of the run.  At each report step
+    in `at` the accelerator reads the block sums (lbf_block_sums, kept on the
+    device), estimates M per block from q and the block pressure gradient
+    (least squares over the three components), solves the upscaled problem
+    for the steady block pressure (darcy_pressure_device, geometric face
+    means) and adds the difference as a density change at unchanged momentum
+    (lbf_add_density).  Mass is conserved and the lattice Boltzmann fixed
+    point is unchanged, so the converged answer is the solver's own; only
+    the slow modes are shortened.  3-D, force along +x; grid edges must be
+    multiples of the block edge."""
 
-    def __init__(self, engine, fluid, g, rho0=1.0, block=8, at=(1000,)):
-        self.engine, self.g, self.rho0, self.b = engine, g, rho0, block
+    def __init__(self, engine, fluid, g, rho0=1.0, block=2, at=(500,), rtol=1e-3, face='geometric', omega=1.0):
+        """at: report steps to correct at, each an int (uses `block`) or a
+        (step, block) pair.  rtol: relative residual at which the block
+        pressure solve stops (the mobility estimate is far coarser).  face:
+        block-face mobility average; omega: fraction of the pressure
+        difference applied."""
+        self.engine, self.g, self.rho0 = engine, g, rho0
         self.fluid = fluid.double()
-        self.at = set(int(t) for t in at)
+        self.at = {}
+        for item in at:
+            t, b = item if isinstance(item, (tuple, list)) else (item, block)
+            self.at[int(t)] = int(b)
+        self.rtol, self.face, self.omega = rtol, face, omega
         self.applied = []
+        self.iterations = []
+        self.seconds = 0.0
 
     def __call__(self, t):
         if t not in self.at:
             return False
-        self.apply()
+        t0 = time.perf_counter()
+        self.apply(self.at[t])
+        torch.cuda.synchronize(self.fluid.device)
+        self.seconds += time.perf_counter() - t0
         self.applied.append(t)
         return True
 
-    def apply(self):
-        b, g, rho0 = self.b, self.g, self.rho0
+    def apply(self, b):
+        g, rho0 = self.g, self.rho0
         dev = self.fluid.device
-        s = torch.from_numpy(self.engine.block_sums(b)).to(dev)
+        D, H, W = self.fluid.shape
+        s = torch.empty(D // b, H // b, W // b, 5, dtype=torch.float64, device=dev)
+        self.engine.block_sums(b, out=s)
         cnt = s[..., 4]
         rho_b = torch.where(cnt > 0, s[..., 0] / cnt.clamp(min=1.0), torch.full_like(cnt, rho0))
         q = s[..., 1:4] / float(b ** 3)
@@ -357,10 +507,15 @@ class DarcyAccelerator:
         den = sum(d * d for d in drive)
         mob = torch.where(den > 0, num / den.clamp(min=1e-300), torch.zeros_like(num))
         mob = torch.clamp(mob, min=1e-3 * float(mob.clamp(min=0).mean()) + 1e-30)
-        target = darcy_pressure(mob, g, b)
+        if mob.is_cuda and self.face == 'geometric':
+            target, it = darcy_pressure_device(mob, g, b, rtol=self.rtol)
+        else:
+            target = darcy_pressure(mob, g, b, rtol=self.rtol, face=self.face)
+            it = _solve_periodic.iterations
+        self.iterations.append(it)
         porous = cnt > 0
         cur = phi - (phi * porous).sum() / porous.sum().clamp(min=1)
-        dphi = (target - cur) * porous
+        dphi = self.omega * (target - cur) * porous
         drho = 3.0 * rho0 * _upsample_periodic(dphi, b) * self.fluid
         drho = drho - drho.sum() / self.fluid.sum().clamp(min=1.0) * self.fluid
         self.engine.add_density(drho.float().contiguous())

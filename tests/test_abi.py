@@ -62,3 +62,24 @@ def test_null_arguments():
     assert lib.lbf_create(None, None, None, None) == -1
     assert lib.lbf_step(None, 1, 0) == -1
     assert lib.lbf_fluid_nodes(None) == 0
+
+
+def test_darcy_pressure_rejects_bad_arguments():
+    """Argument conversion and validation of lbf_darcy_pressure (no GPU work)."""
+    import lbflow_b200 as L
+    lib = L.library()
+    it = ctypes.c_uint32(7)
+    rc = lib.lbf_darcy_pressure(None, 8, 8, 8, 2.0, 1e-5, 1e-3, 10, None, ctypes.byref(it), None)
+    assert rc == -1 and 'bad arguments' in lib.lbf_last_error(None).decode()
+    rc = lib.lbf_darcy_pressure(ctypes.c_void_p(16), 8, 8, 8, 0.0, 1e-5, 1e-3, 10, ctypes.c_void_p(16),
+                                ctypes.byref(it), None)
+    assert rc == -1
+
+
+def test_engine_block_and_density_entry_points_validate():
+    import lbflow_b200 as L
+    lib = L.library()
+    out = (ctypes.c_double * 5)()
+    assert lib.lbf_block_sums(None, 2, out, 5) == -1
+    assert lib.lbf_add_density(None, None) == -1
+    assert lib.lbf_initialize_equilibrium(None, None, 4, 0) == -1

@@ -148,7 +148,7 @@ def test_darcy_pressure_layered_medium():
     x = (torch.arange(W, dtype=torch.float64) + 0.5) / W
     M = 1.0 + 0.6 * torch.sin(2 * math.pi * x)                     # voxel mobility along x
     mob = ws._block_mean(M.expand(D, H, W)[..., None], b)[..., 0]
-    phi = ws.darcy_pressure(mob, g, b)
+    phi = ws.darcy_pressure(mob, g, b, face='harmonic')
     mf = 2 * mob * torch.roll(mob, -1, 2) / (mob + torch.roll(mob, -1, 2))
     face = mf * (g - (torch.roll(phi, -1, 2) - phi) / b)            # x flux through each + face
     assert float(face.std() / face.mean()) < 1e-8
@@ -164,7 +164,7 @@ def test_darcy_pressure_layered_medium():
     # The flux form gives the same pressure from the local response M g.
     q = torch.zeros(D // b, H // b, W // b, 3, dtype=torch.float64)
     q[..., 0] = mob * g
-    phi2 = ws.darcy_pressure_from_flux(q, mob, b)
+    phi2 = ws.darcy_pressure_from_flux(q, mob, b, face='harmonic')
     assert float((phi2 - phi).norm() / phi.norm()) < 0.05
 
 
@@ -174,14 +174,14 @@ def test_darcy_pressure_removes_divergence_3d():
     q = torch.rand(6, 8, 10, 3, generator=gen, dtype=torch.float64) * 1e-5
     mob = 0.5 + torch.rand(6, 8, 10, generator=gen, dtype=torch.float64)
     b = 8
-    phi = ws.darcy_pressure_from_flux(q, mob, b)
+    phi = ws.darcy_pressure_from_flux(q, mob, b, face='harmonic')
     div = torch.zeros_like(mob)
     for c, ax in enumerate((2, 1, 0)):
         nb = torch.roll(mob, -1, ax)
         mf = 2 * mob * nb / (mob + nb)
         face = 0.5 * (q[..., c] + torch.roll(q[..., c], -1, ax)) - mf * (torch.roll(phi, -1, ax) - phi) / b
         div += (face - torch.roll(face, 1, ax)) / b
-    assert float(div.abs().max()) < 1e-9 * float(q.abs().max()) / b
+    assert float(div.abs().max()) < 1e-6 * float(q.abs().max()) / b     # CG stops at 1e-8 relative
     assert abs(float(phi.mean())) < 1e-18
 
 
@@ -197,3 +197,38 @@ def test_upsample_periodic_reproduces_linear_and_constant_fields():
     up = ws._upsample_periodic(phi, b)
     xv = torch.arange(w * b, dtype=torch.float64)
     assert float((up[0, 0] - torch.cos(2 * math.pi * xv / (w * b))).abs().max()) < 0.02
+
+
+def test_smooth121_removes_grid_scale_mode():
+    from lbflow_b200 import warmstart as ws
+    D, H, W = 8, 6, 10
+    z, y, x = torch.meshgrid(torch.arange(D), torch.arange(H), torch.arange(W), indexing='ij')
+    m = torch.ones(D, H, W, dtype=torch.float64)
+    stag = ((-1.0) ** (x + y + z)).double()
+    assert float(ws._smooth121(stag, m).abs().max()) < 1e-12
+    smooth = torch.cos(2 * math.pi * x.double() / W)
+    expect = smooth * (0.5 + 0.5 * math.cos(2 * math.pi / W))
+    assert float((ws._smooth121(smooth, m) - expect).abs().max()) < 1e-12
+    # Solid voxels stay zero and a constant field over the pores is kept.
+    m[2:4, 2:4, 2:4] = 0
+    out = ws._smooth121(torch.full((D, H, W), 3.0, dtype=torch.float64), m)
+    assert torch.allclose(out[m > 0], torch.tensor(3.0, dtype=torch.float64)) and float(out[m == 0].abs().max()) == 0
+
+
+def test_multigrid_transfers_are_adjoint_and_solver_converges():
+    """The V-cycle's restriction is the adjoint of its prolongation / 8 (so the
+    preconditioner is symmetric), and the preconditioned solve of a
+    high-contrast mobility field converges in a few dozen iterations."""
+    from lbflow_b200 import warmstart as ws
+    gen = torch.Generator().manual_seed(1)
+    e = torch.randn(4, 6, 8, generator=gen, dtype=torch.float64)
+    r = torch.randn(8, 12, 16, generator=gen, dtype=torch.float64)
+    assert math.isclose(float((ws._prolong(e) * r).sum()), float(8 * (e * ws._restrict(r)).sum()), rel_tol=1e-12)
+    mob = torch.exp(2.0 * torch.randn(16, 16, 32, generator=gen, dtype=torch.float64))
+    mob[torch.rand(16, 16, 32, generator=gen) < 0.3] = 1e-4
+    phi = ws.darcy_pressure(mob, 1e-5, 2, rtol=1e-8)
+    assert ws._solve_periodic.iterations < 120
+    mf = ws._face_mobility(mob)
+    rhs = 1e-5 * (mf[0] - torch.roll(mf[0], 1, 2)) / 2
+    res = ws._apply(phi, mf, 2.0) - (rhs - rhs.mean())
+    assert float(res.norm() / rhs.norm()) < 1e-7
