@@ -218,7 +218,7 @@ def main():
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--mode', default='mlups', choices=('mlups', 'ttp'),
                     help='mlups: the throughput line; ttp: time to permeability, plain FP64 vs reduced storage')
-    ap.add_argument('--storages', default='fp64,bfp16,fp16,fp32')
+    ap.add_argument('--storages', default='fp64,fp32,fp32+acc,bfp16+acc,fp32+warm0')
     ap.add_argument('--max-steps', type=int, default=400000)
     ap.add_argument('--workload', default='scsp', choices=('scsp', 'color', 'batch', 'operator'),
                     help='scsp: 256^3 single-phase cube; color: 128x128x256 two-phase color-gradient MRT; '
@@ -228,6 +228,9 @@ def main():
     ap.add_argument('--ttp-media', default='cube', choices=('cube', 'eval192'),
                     help='ttp: the 256^3 cube, or held-out 192^3 media')
     ap.add_argument('--seeds', type=int, default=8, help='ttp eval192: number of media')
+    ap.add_argument('--media-index', default=None, help='ttp eval192: comma-separated media indices instead')
+    ap.add_argument('--op-conv-only', action='store_true', help='operator: only the single-convolution roofline '
+                                                                 '(3 warm-up + 20 timed launches)')
     ap.add_argument('--report', type=int, default=1000, help='ttp: report interval in steps')
     ap.add_argument('--block', type=int, default=2, help='ttp: block edge of the Darcy corrections (warm start, +acc)')
     ap.add_argument('--accel-at', default='500', help='ttp: report steps (step or step:block, comma separated) at '
@@ -457,7 +460,8 @@ def ttp_media(args):
         return [dict(name=f'cube{args.size}', geometry=make_geometry(args.size, 3.0, 0.22, seed=0),
                      sigma=3.0, porosity=0.22, seed=0)]
     out = []
-    for k in range(args.seeds):
+    pick = [int(v) for v in args.media_index.split(',')] if args.media_index else range(args.seeds)
+    for k in pick:
         seed = 900000 + k
         rng = np.random.default_rng([seed, 5])
         sigma, por = float(rng.uniform(2.0, 5.0)), float(rng.uniform(0.15, 0.30))
@@ -488,10 +492,26 @@ def time_to_permeability(args):
     if any('+warm' in r or '+flux' in r or '+rho' in r for r in args.storages.split(',')):
         net, wmeta = ws.load(args.warm_weights)
     # One-time process set-up outside the timed runs (as CUDA context creation
-    # is): the block pressure solver's kernels loaded on a small problem.
-    ws.darcy_pressure_device(torch.ones(8, 8, 8, dtype=torch.float64, device='cuda'), 1e-5, 2)
-    torch.cuda.synchronize()
+    # is): the block pressure solver's and interpolation kernels loaded, and
+    # the allocator grown, on a zero problem of each medium's block grid.
     media = ttp_media(args)
+    for med in media:
+        nz, ny, nx = med['geometry'].shape
+        b = args.block
+        ws.darcy_pressure_device(torch.ones(nz // b, ny // b, nx // b, dtype=torch.float64, device='cuda'), 1e-5, b)
+        ws._upsample_periodic(torch.zeros(nz // b, ny // b, nx // b, dtype=torch.float64, device='cuda'), b)
+    # Kernels of every storage's step, block sums and density increment are
+    # loaded on first launch; launch them once on a 16^3 medium.
+    tiny = make_geometry(16, 2.0, 0.35, seed=1)
+    tiny_fluid = torch.from_numpy(tiny != 255).cuda()
+    for storage in sorted({n.split('+')[0] for n in args.storages.split(',')}):
+        with Engine(tiny, LABELS, model='scsp', collision=args.collision, tau=(1.0,), storage=storage) as e:
+            e.initialize()
+            e.step(1, macros=True)
+            ws.DarcyAccelerator(e, tiny_fluid, 1e-5, block=2, at=(1,))(1)
+            e.step(1)
+            e.check()
+    torch.cuda.synchronize()
     results = []
     for med in media:
         geometry = med['geometry']
@@ -585,19 +605,23 @@ def operator_run(args):
         y = net(x)
         (y.float() * R.float()).sum().backward()
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
     steps = max(5, min(args.steps, 50))
-    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(0) as clocks:
-        t0.record()
-        for _ in range(steps):
+    ms = float('nan')
+    clocks = None
+    if not args.op_conv_only:
+        for _ in range(args.warmup):
             step()
-        t1.record()
         torch.cuda.synchronize()
-    conv.check()
-    ms = t0.elapsed_time(t1) / steps
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(0) as clk:
+            t0.record()
+            for _ in range(steps):
+                step()
+            t1.record()
+            torch.cuda.synchronize()
+        clocks = clk.summary()
+        conv.check()
+        ms = t0.elapsed_time(t1) / steps
     # Heaviest single launch: 64 -> 64 channel 3x3x3 conv at 2 x 48^3 (level 3 of a 192^3 input).
     xa = torch.randn(2, 48, 48, 48, 64, device='cuda').to(torch.bfloat16)
     w = torch.randn(64, 64, 3, 3, 3, device='cuda') * 0.05
@@ -623,7 +647,7 @@ def operator_run(args):
                           roofline=dict(bound='tensor', achieved=achieved, peak=peak, unit='TFLOP/s',
                                         frac=achieved / peak, traffic=None, peak_kind='measured burst bf16',
                                         kernel='igemm conv3 64->64 at 2x48^3 (forward)', launch_ms=launch_ms),
-                          gpu_launches=None, clocks=clocks.summary())))
+                          gpu_launches=None, clocks=clocks)))
     return 0
 
 def end_to_end(geometry, args, device):
