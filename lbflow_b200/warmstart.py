@@ -601,7 +601,7 @@ def train(net, samples, iters=2000, lr=2e-3, batch_voxels=2 * 64 ** 3, seed=0, l
         torch.nn.utils.clip_grad_norm_(net.parameters(), 1.0)
         opt.step()
         if it % 50 == 0 or it == iters - 1:
-            lv = float(loss)
+            lv = float(loss.detach())
             hist.append((it, lv, time.perf_counter() - t0))
             if log:
                 log(f'iter {it} loss {lv:.4e} shape {shp} batch {nb} {time.perf_counter() - t0:.1f}s')
