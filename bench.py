@@ -479,7 +479,8 @@ def time_to_permeability(args):
     network inference and the block-scale Darcy pressure with --block voxel
     blocks, inside the timed region); '+warmB' sets the block edge B (0: the
     network's fields only); '+fluxB' uses the flux-divergence correction
-    instead; '+rhoB' starts from rest with the predicted density only;
+    instead; warm starts set the predicted density only ('+warmvB' also the
+    predicted velocity);
     '+accB' applies the in-run block Darcy correction
     (warmstart.DarcyAccelerator) at the --accel-at report steps.
     K = nu <u_x> / g."""
@@ -489,7 +490,7 @@ def time_to_permeability(args):
     torch.cuda.set_device(0)
     net = None
     from lbflow_b200 import warmstart as ws
-    if any('+warm' in r or '+flux' in r or '+rho' in r for r in args.storages.split(',')):
+    if any(m in r for r in args.storages.split(',') for m in ('+warm', '+flux', '+rho')):
         net, wmeta = ws.load(args.warm_weights)
     # One-time process set-up outside the timed runs (as CUDA context creation
     # is): the block pressure solver's and interpolation kernels loaded, and
@@ -498,7 +499,8 @@ def time_to_permeability(args):
     for med in media:
         nz, ny, nx = med['geometry'].shape
         b = args.block
-        ws.darcy_pressure_device(torch.ones(nz // b, ny // b, nx // b, dtype=torch.float64, device='cuda'), 1e-5, b)
+        mob = torch.rand(nz // b, ny // b, nx // b, dtype=torch.float64, device='cuda') + 0.5
+        ws.darcy_pressure_device(mob, 1e-5, b)
         ws._upsample_periodic(torch.zeros(nz // b, ny // b, nx // b, dtype=torch.float64, device='cuda'), b)
     # Kernels of every storage's step, block sums and density increment are
     # loaded on first launch; launch them once on a 16^3 medium.
@@ -525,9 +527,9 @@ def time_to_permeability(args):
             for mod in mods:
                 kind = mod.rstrip('0123456789')
                 block = int(mod[len(kind):]) if mod[len(kind):] else args.block
-                if kind in ('warm', 'flux', 'rho'):
-                    mode = {'warm': 'darcy', 'flux': 'flux', 'rho': 'none'}[kind] if block else 'none'
-                    start = (lambda b=block, m=mode, v=(kind != 'rho'):
+                if kind in ('warm', 'warmv', 'flux', 'rho'):
+                    mode = {'warm': 'darcy', 'warmv': 'darcy', 'flux': 'flux', 'rho': 'none'}[kind] if block else 'none'
+                    start = (lambda b=block, m=mode, v=(kind == 'warmv'):
                              ws.warm_start(eng, net, fluid, 1.0, 1e-5, block=b, mode=m, velocity=v))
                 elif kind == 'acc':
                     sched = [tuple(int(v) for v in item.split(':')) if ':' in item else int(item)

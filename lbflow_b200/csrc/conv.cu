@@ -76,16 +76,6 @@ __device__ __forceinline__ int wrap(int v, int n) {
     return v < 0 ? v + n : (v >= n ? v - n : v);
 }
 
-// Address of the 8 channels [ch, ch+8) of tap (dz,dy,dx) of row voxel c.
-__device__ __forceinline__ const uint16_t* gather_ptr(const Gather& g, const Coord& c, int dz, int dy, int dx,
-                                                      uint32_t ch) {
-    const int z = wrap(int(g.stride) * c.z + dz - g.pad, int(g.in_d));
-    const int y = wrap(int(g.stride) * c.y + dy - g.pad, int(g.in_h));
-    const int x = wrap(int(g.stride) * c.x + dx - g.pad, int(g.in_w));
-    const size_t vox = ((size_t(c.b) * g.in_d + z) * g.in_h + y) * g.in_w + x;
-    return ch < g.c0 ? g.src0 + vox * g.c0 + ch : g.src1 + vox * g.c1 + (ch - g.c0);
-}
-
 __device__ __forceinline__ void tap_offsets(const Gather& g, uint32_t tap, int& dz, int& dy, int& dx) {
     const uint32_t k2 = g.ks * g.ks;
     dz = int(tap / k2);
@@ -202,47 +192,84 @@ struct IgemmArgs {
     uint32_t* err;
 };
 
+// Voxel index of tap (dz, dy, dx) of row voxel c, and the address of channels
+// [ch, ch + 8) of that voxel in whichever source holds them.
+__device__ __forceinline__ size_t gather_vox(const Gather& g, const Coord& c, int dz, int dy, int dx) {
+    const int z = wrap(int(g.stride) * c.z + dz - g.pad, int(g.in_d));
+    const int y = wrap(int(g.stride) * c.y + dy - g.pad, int(g.in_h));
+    const int x = wrap(int(g.stride) * c.x + dx - g.pad, int(g.in_w));
+    return ((size_t(c.b) * g.in_d + z) * g.in_h + y) * g.in_w + x;
+}
+__device__ __forceinline__ const uint16_t* chan_ptr(const Gather& g, size_t vox, uint32_t ch) {
+    return ch < g.c0 ? g.src0 + vox * g.c0 + ch : g.src1 + vox * g.c1 + (ch - g.c0);
+}
+
+// A tile: thread t owns tile row t and copies its 8 16-byte pieces of each
+// 64-wide K stage.  When a stage lies inside one tap of one source (channel
+// counts multiples of 64) the row's 128 bytes are contiguous in memory: one
+// address per stage.  Otherwise the tap and channel advance piece by piece.
 template <int BN>
 struct IgemmLoader {
     const IgemmArgs& p;
     SmemRing r;
-    Coord rc[8];          // rows (t >> 3) + 16 i of the tile
-    bool rv[8];
+    Coord rc;
+    bool rv;
+    bool uniform;
     uint32_t n0;
-    uint32_t poff;        // swizzled byte offset of this thread's 16-byte piece
+    uint32_t sw;          // swizzle of the thread's row (row mod 8)
+    uint32_t poff_b;      // swizzled byte offset of the thread's B piece
 
     __device__ IgemmLoader(const IgemmArgs& a, const SmemRing& ring, uint32_t m0, uint32_t n0_)
         : p(a), r(ring), n0(n0_) {
         const uint32_t t = threadIdx.x;
-        poff = (((t & 7u) ^ ((t >> 3) & 7u)) << 4);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const uint32_t m = m0 + (t >> 3) + 16u * i;
-            rv[i] = m < p.g.rows;
-            rc[i] = row_coord(p.g, rv[i] ? m : 0u);
-        }
+        const uint32_t m = m0 + t;
+        rv = m < p.g.rows;
+        rc = row_coord(p.g, rv ? m : 0u);
+        sw = t & 7u;
+        poff_b = (((t & 7u) ^ ((t >> 3) & 7u)) << 4);
+        uniform = (p.g.ct % kBK == 0) && (p.g.c1 == 0 || p.g.c0 % kBK == 0);
     }
 
     __device__ void load(uint32_t chunk, int s) {
         const uint32_t t = threadIdx.x;
-        const uint32_t k0 = chunk * kBK + (t & 7u) * 8u;
-        const uint32_t tap = k0 / p.g.ct;
-        const uint32_t ch = k0 - tap * p.g.ct;
-        const bool kv = tap < p.g.taps;
-        int dz = 0, dy = 0, dx = 0;
-        if (kv) tap_offsets(p.g, tap, dz, dy, dx);
-        const uint32_t a = r.a(s) + (t >> 3) * 128u + poff;
+        const uint32_t a = r.a(s) + t * 128u;
+        uint32_t k = chunk * kBK;
+        uint32_t tap = k / p.g.ct;
+        uint32_t ch = k - tap * p.g.ct;
+        if (uniform) {
+            const bool v = rv && tap < p.g.taps;
+            const uint16_t* src = p.g.src0;
+            if (v) {
+                int dz, dy, dx;
+                tap_offsets(p.g, tap, dz, dy, dx);
+                src = chan_ptr(p.g, gather_vox(p.g, rc, dz, dy, dx), ch);
+            }
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const bool v = kv && rv[i];
-            const uint16_t* src = v ? gather_ptr(p.g, rc[i], dz, dy, dx, ch) : p.g.src0;
-            cp_async16(a + uint32_t(i) * 16u * 128u, src, v ? 16u : 0u);
+            for (uint32_t j = 0; j < 8; ++j)
+                cp_async16(a + ((j ^ sw) << 4), v ? src + 8u * j : p.g.src0, v ? 16u : 0u);
+        } else {
+            uint32_t cur = 0xffffffffu;
+            size_t vox = 0;
+#pragma unroll
+            for (uint32_t j = 0; j < 8; ++j) {
+                const bool v = rv && tap < p.g.taps;
+                if (v && tap != cur) {
+                    int dz, dy, dx;
+                    tap_offsets(p.g, tap, dz, dy, dx);
+                    vox = gather_vox(p.g, rc, dz, dy, dx);
+                    cur = tap;
+                }
+                cp_async16(a + ((j ^ sw) << 4), v ? chan_ptr(p.g, vox, ch) : p.g.src0, v ? 16u : 0u);
+                ch += 8u;
+                if (ch >= p.g.ct) { ch = 0; ++tap; }
+            }
         }
-        const uint32_t b = r.b(s) + (t >> 3) * 128u + poff;
+        const uint32_t kb = chunk * kBK + (t & 7u) * 8u;
+        const uint32_t b = r.b(s) + (t >> 3) * 128u + poff_b;
 #pragma unroll
         for (int i = 0; i < BN / 16; ++i) {
             const uint32_t n = (t >> 3) + 16u * i;
-            cp_async16(b + uint32_t(i) * 16u * 128u, p.w + size_t(n0 + n) * p.k_pad + k0, 16u);
+            cp_async16(b + uint32_t(i) * 16u * 128u, p.w + size_t(n0 + n) * p.k_pad + kb, 16u);
         }
     }
     __device__ uint64_t adesc(int s, int kk) const { return desc_sw128(r.a(s) + 32u * kk, 16u, 1024u); }
@@ -357,73 +384,90 @@ struct WgradLoader {
     const WgradArgs& p;
     SmemRing r;
     Step64 st;
-    Coord rc[8];          // rows k = (t >> 4) + 8 i of the current chunk
-    uint32_t m[8];
+    Coord rc;             // voxel of this thread's K row of the current chunk
+    uint32_t base;        // first row of the current chunk
     uint32_t m_end;
-    int dz, dy, dx;
-    uint32_t ch;
-    bool iv;
-    uint32_t aoff;        // byte offset of this thread's A pieces inside a stage
+    uint32_t kr, half;    // K row (t >> 1) and which 8 of its 16 pieces (t & 1)
+    uint32_t tap0, ch0;   // tap and channel of the thread's first piece
+    bool uniform;         // its 8 pieces are 64 contiguous channels of one tap and source
+    uint32_t aoff;        // byte offset of the thread's first A piece inside a stage
     uint32_t j0;
 
     __device__ WgradLoader(const WgradArgs& a, const SmemRing& ring, uint32_t i0, uint32_t j0_, uint32_t c_begin,
                            uint32_t m_end_, const Step64& s64)
         : p(a), r(ring), st(s64), m_end(m_end_), j0(j0_) {
         const uint32_t t = threadIdx.x;
-        const uint32_t pc = t & 15u, kr = (t >> 4) & 7u;
-        const uint32_t i = i0 + pc * 8u;
-        const uint32_t tap = i / p.g.ct;
-        ch = i - tap * p.g.ct;
-        iv = tap < p.g.taps;
-        dz = dy = dx = 0;
-        if (iv) tap_offsets(p.g, tap, dz, dy, dx);
-        aoff = (pc >> 3) * 1024u + kr * 128u + (((pc & 7u) ^ kr) << 4);
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            m[q] = c_begin * kBK + (t >> 4) + 8u * q;
-            rc[q] = row_coord(p.g, m[q] < m_end ? m[q] : 0u);
-        }
+        kr = t >> 1;
+        half = t & 1u;
+        const uint32_t i = i0 + half * 64u;
+        tap0 = i / p.g.ct;
+        ch0 = i - tap0 * p.g.ct;
+        uniform = (p.g.ct % kBK == 0) && (p.g.c1 == 0 || p.g.c0 % kBK == 0);
+        aoff = half * 1024u + (kr >> 3) * 2048u + (kr & 7u) * 128u;
+        base = c_begin * kBK;
+        const uint32_t m = base + kr;
+        rc = row_coord(p.g, m < m_end ? m : 0u);
     }
 
     __device__ void advance() {
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            m[q] += kBK;
-            Coord& c = rc[q];
-            c.x += st.ax;
-            int carry = c.x >= int(p.g.out_w);
-            if (carry) c.x -= int(p.g.out_w);
-            c.y += st.ay + carry;
-            carry = c.y >= int(p.g.out_h);
-            if (carry) c.y -= int(p.g.out_h);
-            c.z += st.az + carry;
-            carry = c.z >= int(p.g.out_d);
-            if (carry) c.z -= int(p.g.out_d);
-            c.b += st.ab + carry;
-        }
+        base += kBK;
+        rc.x += st.ax;
+        int carry = rc.x >= int(p.g.out_w);
+        if (carry) rc.x -= int(p.g.out_w);
+        rc.y += st.ay + carry;
+        carry = rc.y >= int(p.g.out_h);
+        if (carry) rc.y -= int(p.g.out_h);
+        rc.z += st.az + carry;
+        carry = rc.z >= int(p.g.out_d);
+        if (carry) rc.z -= int(p.g.out_d);
+        rc.b += st.ab + carry;
     }
 
     __device__ void load(uint32_t /*chunk*/, int s) {
         const uint32_t t = threadIdx.x;
         const uint32_t a = r.a(s) + aoff;
+        const uint32_t sw = kr & 7u;
+        const bool rowv = base + kr < m_end;
+        if (uniform) {
+            const bool v = rowv && tap0 < p.g.taps;
+            const uint16_t* src = p.g.src0;
+            if (v) {
+                int dz, dy, dx;
+                tap_offsets(p.g, tap0, dz, dy, dx);
+                src = chan_ptr(p.g, gather_vox(p.g, rc, dz, dy, dx), ch0);
+            }
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const bool v = iv && m[q] < m_end;
-            const uint16_t* src = v ? gather_ptr(p.g, rc[q], dz, dy, dx, ch) : p.g.src0;
-            cp_async16(a + uint32_t(q) * 2048u, src, v ? 16u : 0u);
+            for (uint32_t jj = 0; jj < 8; ++jj)
+                cp_async16(a + ((jj ^ sw) << 4), v ? src + 8u * jj : p.g.src0, v ? 16u : 0u);
+        } else {
+            uint32_t tap = tap0, ch = ch0, cur = 0xffffffffu;
+            size_t vox = 0;
+#pragma unroll
+            for (uint32_t jj = 0; jj < 8; ++jj) {
+                const bool v = rowv && tap < p.g.taps;
+                if (v && tap != cur) {
+                    int dz, dy, dx;
+                    tap_offsets(p.g, tap, dz, dy, dx);
+                    vox = gather_vox(p.g, rc, dz, dy, dx);
+                    cur = tap;
+                }
+                cp_async16(a + ((jj ^ sw) << 4), v ? chan_ptr(p.g, vox, ch) : p.g.src0, v ? 16u : 0u);
+                ch += 8u;
+                if (ch >= p.g.ct) { ch = 0; ++tap; }
+            }
         }
         // B: BN/8 pieces per K row.
         constexpr uint32_t kPieces = BN / 8;
         constexpr uint32_t kRowsPerPass = kThreads / kPieces;
         constexpr uint32_t kSbo = (BN / 64) * 1024u;
         const uint32_t qn = t % kPieces;
-        const uint32_t jj = j0 + qn * 8u;
+        const uint32_t jn = j0 + qn * 8u;
 #pragma unroll
         for (uint32_t it = 0; it < kBK / kRowsPerPass; ++it) {
             const uint32_t k = t / kPieces + kRowsPerPass * it;
-            const uint32_t row = m[0] - (t >> 4) + k;        // chunk base + k
-            const bool v = row < m_end && jj < p.cb;
-            const uint16_t* src = v ? p.b + size_t(row) * p.cb + jj : p.b;
+            const uint32_t row = base + k;
+            const bool v = row < m_end && jn < p.cb;
+            const uint16_t* src = v ? p.b + size_t(row) * p.cb + jn : p.b;
             const uint32_t dst = r.b(s) + (qn >> 3) * 1024u + (k >> 3) * kSbo + (k & 7u) * 128u +
                                  (((qn & 7u) ^ (k & 7u)) << 4);
             cp_async16(dst, src, v ? 16u : 0u);

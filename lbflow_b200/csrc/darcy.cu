@@ -28,6 +28,7 @@
 namespace {
 
 constexpr int kT = 256;
+constexpr int kCoarseSweeps = 120;   // Jacobi sweeps on the coarsest (<= 1024-cell) grid
 
 struct Dims {
     int nz, ny, nx;
@@ -275,13 +276,19 @@ __global__ void dot_partial(size_t n, const double* __restrict__ a, const double
     }
     if (threadIdx.x == 0) part[blockIdx.x] = s[0];
 }
+// Second pass: one block sums the partials in a fixed tree order.
 __global__ void dot_final(int nb, const double* __restrict__ part, double* __restrict__ out)
 {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        double s = 0.0;
-        for (int i = 0; i < nb; ++i) s += part[i];
-        out[0] = s;
+    __shared__ double s[kT];
+    double v = 0.0;
+    for (int i = threadIdx.x; i < nb; i += kT) v += part[i];
+    s[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = kT / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) s[threadIdx.x] += s[threadIdx.x + o];
+        __syncthreads();
     }
+    if (threadIdx.x == 0) out[0] = s[0];
 }
 __global__ void copy_scalar(const double* __restrict__ a, double* __restrict__ b) { b[0] = a[0]; }
 __global__ void sub_mean(size_t n, const double* __restrict__ sum, double* __restrict__ a)
@@ -301,19 +308,21 @@ struct Level {
 struct Solver {
     cudaStream_t s = nullptr;
     std::vector<Level> L;
-    std::vector<void*> allocs;
     double* part = nullptr;
     int nb_dot = 0;
     cudaError_t err = cudaSuccess;
+    // One device allocation carved into 256-byte-aligned arrays: a first
+    // pass (base == nullptr) only adds up the size.
+    char* base = nullptr;
+    size_t used = 0;
 
     template <class T> T* alloc(size_t n)
     {
-        void* p = nullptr;
-        if (err == cudaSuccess) err = cudaMalloc(&p, n * sizeof(T));
-        if (p) allocs.push_back(p);
-        return static_cast<T*>(p);
+        T* p = base ? reinterpret_cast<T*>(base + used) : nullptr;
+        used += (n * sizeof(T) + 255) / 256 * 256;
+        return p;
     }
-    ~Solver() { for (void* p : allocs) cudaFree(p); }
+    ~Solver() { if (base) cudaFree(base); }
 
     void smooth(int l, int sweeps)
     {
@@ -329,7 +338,7 @@ struct Solver {
     {
         Level& v = L[l];
         if (l + 1 == (int)L.size()) {
-            coarse_solve<<<1, 1024, 0, s>>>(v.d, v.h2inv, 400, v.r, v.mx, v.my, v.mz, v.x);
+            coarse_solve<<<1, 1024, 0, s>>>(v.d, v.h2inv, kCoarseSweeps, v.r, v.mx, v.my, v.mz, v.x);
             return;
         }
         fill0<<<nblk(v.d.n()), kT, 0, s>>>(v.d.n(), v.x);
@@ -345,7 +354,7 @@ struct Solver {
     void dot(size_t n, const double* a, const double* b, double* out)
     {
         dot_partial<<<nb_dot, kT, 0, s>>>(n, a, b, part);
-        dot_final<<<1, 32, 0, s>>>(nb_dot, part, out);
+        dot_final<<<1, kT, 0, s>>>(nb_dot, part, out);
     }
 };
 
@@ -378,27 +387,37 @@ extern "C" int lbf_darcy_pressure(const double* mob, uint32_t nz, uint32_t ny, u
     }
     Solver S;
     S.s = static_cast<cudaStream_t>(stream);
-    float hh = (float)h;
-    for (const Dims& d : dims) {
-        Level v{};
-        v.d = d;
-        v.h2inv = 1.0f / (hh * hh);
-        const size_t m = d.n();
-        v.mx = S.alloc<float>(m); v.my = S.alloc<float>(m); v.mz = S.alloc<float>(m);
-        v.x = S.alloc<float>(m); v.r = S.alloc<float>(m); v.t = S.alloc<float>(m);
-        S.L.push_back(v);
-        hh *= 2.f;
-    }
-    double* rhs = S.alloc<double>(n);
-    double* r = S.alloc<double>(n);
-    double* z = S.alloc<double>(n);
-    double* p = S.alloc<double>(n);
-    double* Ap = S.alloc<double>(n);
-    double* sc = S.alloc<double>(8);          // scalars: rz, pAp, rz_new, rr, sum
     S.nb_dot = (int)std::min<size_t>(nblk(n), 1184);
-    S.part = S.alloc<double>(S.nb_dot);
-    if (S.err != cudaSuccess)
-        return fail(std::string("lbf_darcy_pressure: ") + cudaGetErrorString(S.err), LBF_ENOMEM);
+    double *rhs = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *Ap = nullptr, *sc = nullptr;
+    for (int pass = 0; pass < 2; ++pass) {
+        if (pass == 1) {
+            void* mem = nullptr;
+            S.err = cudaMalloc(&mem, S.used);
+            if (S.err != cudaSuccess)
+                return fail(std::string("lbf_darcy_pressure: ") + cudaGetErrorString(S.err), LBF_ENOMEM);
+            S.base = static_cast<char*>(mem);
+            S.used = 0;
+            S.L.clear();
+        }
+        float hh = (float)h;
+        for (const Dims& d : dims) {
+            Level v{};
+            v.d = d;
+            v.h2inv = 1.0f / (hh * hh);
+            const size_t m = d.n();
+            v.mx = S.alloc<float>(m); v.my = S.alloc<float>(m); v.mz = S.alloc<float>(m);
+            v.x = S.alloc<float>(m); v.r = S.alloc<float>(m); v.t = S.alloc<float>(m);
+            S.L.push_back(v);
+            hh *= 2.f;
+        }
+        rhs = S.alloc<double>(n);
+        r = S.alloc<double>(n);
+        z = S.alloc<double>(n);
+        p = S.alloc<double>(n);
+        Ap = S.alloc<double>(n);
+        sc = S.alloc<double>(8);          // scalars: rz, pAp, rz_new, rr, sum
+        S.part = S.alloc<double>(S.nb_dot);
+    }
     cudaStream_t s = S.s;
     const double h2inv = 1.0 / (h * h);
     setup_fine<<<nblk(n), kT, 0, s>>>(d0, mob, g, h, S.L[0].mx, S.L[0].my, S.L[0].mz, rhs);

@@ -391,7 +391,7 @@ def _smooth121(x, m):
     return torch.where(den > 0, num / den.clamp(min=1e-30), torch.zeros_like(num)) * m
 
 
-def predict(net, fluid, tau, g, rho0=1.0, block=8, mode='darcy', velocity=True, smooth=True):
+def predict(net, fluid, tau, g, rho0=1.0, block=8, mode='darcy', velocity=False, smooth=True):
     """Warm-start fields (D, H, W, 4) float32 on the GPU: velocity x, y, z and
     density for force g along +x and relaxation time tau.
 
@@ -401,8 +401,12 @@ def predict(net, fluid, tau, g, rho0=1.0, block=8, mode='darcy', velocity=True, 
                   with block mobilities = block means of the network's k_x / nu.
     mode 'flux':  the network's density plus the pressure that makes its
                   block fluxes conservative (darcy_pressure_from_flux).
-    velocity=False starts from rest with the predicted density only (the
-    velocity relaxes to the pressure within the fast viscous transient).
+    velocity=False (the default) starts from rest with the predicted density
+    only: the velocity relaxes to the pressure within the viscous transient
+    of a pore, so a predicted velocity adds nothing to the start, while its
+    residual imperfections excite a period-2 staggered mode that keeps
+    LBFlow's adjacent-step residual above 1e-6 (measured on the 256^3 cube:
+    never converged in 150,000 steps with it, 95,000 steps without).
     smooth: [1, 2, 1] filter of the predicted fields (_smooth121)."""
     with torch.no_grad():
         f = features(fluid.unsqueeze(0))
@@ -437,7 +441,7 @@ def predict(net, fluid, tau, g, rho0=1.0, block=8, mode='darcy', velocity=True, 
         return out.contiguous()
 
 
-def warm_start(engine, net, fluid, tau, g, rho0=1.0, block=8, mode='darcy', velocity=True, smooth=True):
+def warm_start(engine, net, fluid, tau, g, rho0=1.0, block=8, mode='darcy', velocity=False, smooth=True):
     """Initialise `engine` from the network's prediction; returns the fields."""
     fields = predict(net, fluid, tau, g, rho0, block, mode, velocity, smooth)
     torch.cuda.current_stream(fluid.device).synchronize()
