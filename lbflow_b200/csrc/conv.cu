@@ -16,7 +16,7 @@
 //         CTAs with fixed-order partial sums.  Weight gradients run here.
 //
 // Block: 128 threads = one warpgroup; every thread gathers 16-byte pieces
-// with cp.async into a 4-stage ring of 128-byte-swizzled operand tiles,
+// with cp.async into a 3-stage ring of 128-byte-swizzled operand tiles,
 // thread 0 issues four M=128 x N x K=16 MMAs per 64-wide K stage and commits
 // them to the stage's mbarrier; the ring slot is refilled once that barrier
 // fires.  The epilogue reads the accumulator rows back with tcgen05.ld (warp
@@ -41,7 +41,7 @@ using namespace lbf::umma;
 constexpr int kThreads = 128;
 constexpr int kBM = 128;             // tile rows = UMMA M
 constexpr int kBK = 64;              // K per stage: one 128-byte swizzle row of bf16
-constexpr int kStages = 4;
+constexpr int kStages = 3;
 constexpr uint32_t kTileA = kBM * kBK * 2;
 constexpr long long kWaitCycles = 4000000000LL;   // about 2 s at the boost clock
 
@@ -237,6 +237,9 @@ struct IgemmLoader {
         uint32_t tap = k / p.g.ct;
         uint32_t ch = k - tap * p.g.ct;
         if (uniform) {
+            // Each thread finds its row's 128 contiguous bytes; the copies are
+            // then spread so that lanes 8q..8q+7 move the 8 pieces of one row
+            // (coalesced), the row addresses passed by warp shuffles.
             const bool v = rv && tap < p.g.taps;
             const uint16_t* src = p.g.src0;
             if (v) {
@@ -244,9 +247,17 @@ struct IgemmLoader {
                 tap_offsets(p.g, tap, dz, dy, dx);
                 src = chan_ptr(p.g, gather_vox(p.g, rc, dz, dy, dx), ch);
             }
+            const uint32_t lane = t & 31u, wbase = t & ~31u, j = lane & 7u;
+            const unsigned long long sp = reinterpret_cast<unsigned long long>(src);
 #pragma unroll
-            for (uint32_t j = 0; j < 8; ++j)
-                cp_async16(a + ((j ^ sw) << 4), v ? src + 8u * j : p.g.src0, v ? 16u : 0u);
+            for (uint32_t i = 0; i < 8; ++i) {
+                const uint32_t rw = 4u * i + (lane >> 3);              // row within the warp
+                const unsigned long long q = __shfl_sync(0xffffffffu, sp, int(rw));
+                const int vq = __shfl_sync(0xffffffffu, int(v), int(rw));
+                const uint32_t row = wbase + rw;
+                const uint32_t dst = r.a(s) + row * 128u + ((j ^ (row & 7u)) << 4);
+                cp_async16(dst, vq ? reinterpret_cast<const uint16_t*>(q) + 8u * j : p.g.src0, vq ? 16u : 0u);
+            }
         } else {
             uint32_t cur = 0xffffffffu;
             size_t vox = 0;
@@ -429,6 +440,9 @@ struct WgradLoader {
         const uint32_t sw = kr & 7u;
         const bool rowv = base + kr < m_end;
         if (uniform) {
+            // Thread (kr, half) finds 128 contiguous bytes of its K row; the
+            // copies are spread so that lanes 16q..16q+15 move the 16 pieces of
+            // one K row (256 contiguous bytes), addresses passed by shuffles.
             const bool v = rowv && tap0 < p.g.taps;
             const uint16_t* src = p.g.src0;
             if (v) {
@@ -436,9 +450,20 @@ struct WgradLoader {
                 tap_offsets(p.g, tap0, dz, dy, dx);
                 src = chan_ptr(p.g, gather_vox(p.g, rc, dz, dy, dx), ch0);
             }
+            const uint32_t lane = t & 31u, pc = lane & 15u;
+            const unsigned long long sp = reinterpret_cast<unsigned long long>(src);
 #pragma unroll
-            for (uint32_t jj = 0; jj < 8; ++jj)
-                cp_async16(a + ((jj ^ sw) << 4), v ? src + 8u * jj : p.g.src0, v ? 16u : 0u);
+            for (uint32_t i = 0; i < 8; ++i) {
+                const uint32_t rw = 2u * i + (lane >> 4);              // K row within the warp's 16
+                const int from = int(2u * rw + (pc >> 3));             // the thread holding that half
+                const unsigned long long q = __shfl_sync(0xffffffffu, sp, from);
+                const int vq = __shfl_sync(0xffffffffu, int(v), from);
+                const uint32_t k = (t >> 5) * 16u + rw;                // K row within the chunk
+                const uint32_t dst = r.a(s) + (pc >> 3) * 1024u + (k >> 3) * 2048u + (k & 7u) * 128u +
+                                     (((pc & 7u) ^ (k & 7u)) << 4);
+                cp_async16(dst, vq ? reinterpret_cast<const uint16_t*>(q) + 8u * (pc & 7u) : p.g.src0,
+                           vq ? 16u : 0u);
+            }
         } else {
             uint32_t tap = tap0, ch = ch0, cur = 0xffffffffu;
             size_t vox = 0;

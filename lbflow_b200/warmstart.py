@@ -481,6 +481,7 @@ class DarcyAccelerator:
         self.rtol, self.face, self.omega = rtol, face, omega
         self.applied = []
         self.iterations = []
+        self.phases = []          # per correction: seconds of each phase (synchronised)
         self.seconds = 0.0
 
     def __call__(self, t):
@@ -497,8 +498,15 @@ class DarcyAccelerator:
         g, rho0 = self.g, self.rho0
         dev = self.fluid.device
         D, H, W = self.fluid.shape
+        marks = [('start', time.perf_counter())]
+
+        def mark(name):
+            torch.cuda.synchronize(dev)
+            marks.append((name, time.perf_counter()))
+
         s = torch.empty(D // b, H // b, W // b, 5, dtype=torch.float64, device=dev)
         self.engine.block_sums(b, out=s)
+        mark('block_sums')
         cnt = s[..., 4]
         rho_b = torch.where(cnt > 0, s[..., 0] / cnt.clamp(min=1.0), torch.full_like(cnt, rho0))
         q = s[..., 1:4] / float(b ** 3)
@@ -511,18 +519,23 @@ class DarcyAccelerator:
         den = sum(d * d for d in drive)
         mob = torch.where(den > 0, num / den.clamp(min=1e-300), torch.zeros_like(num))
         mob = torch.clamp(mob, min=1e-3 * float(mob.clamp(min=0).mean()) + 1e-30)
+        mark('mobility')
         if mob.is_cuda and self.face == 'geometric':
             target, it = darcy_pressure_device(mob, g, b, rtol=self.rtol)
         else:
             target = darcy_pressure(mob, g, b, rtol=self.rtol, face=self.face)
             it = _solve_periodic.iterations
         self.iterations.append(it)
+        mark('solve')
         porous = cnt > 0
         cur = phi - (phi * porous).sum() / porous.sum().clamp(min=1)
         dphi = self.omega * (target - cur) * porous
         drho = 3.0 * rho0 * _upsample_periodic(dphi, b) * self.fluid
         drho = drho - drho.sum() / self.fluid.sum().clamp(min=1.0) * self.fluid
+        mark('density_field')
         self.engine.add_density(drho.float().contiguous())
+        mark('add_density')
+        self.phases.append({n: round(t - marks[k][1], 4) for k, (n, t) in enumerate(marks[1:])})
 
 
 def save(net, path, meta=None):
