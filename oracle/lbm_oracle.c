@@ -34,6 +34,25 @@ static const int RELD19[3][10] = { {5,11,12,15,16,6,13,14,17,18},
                                    {3,8,7,15,17,4,9,10,16,18},
                                    {1,7,9,11,13,2,8,10,12,14} };
 
+/* Zou-He tables per boundary direction dir = 1..2D (gridspace.cpp:87-91 for
+ * D2Q9, 122-141 for D3Q19): REL[dir] = the directions with the same sign as
+ * dir along its axis, in the reference's order; PERP[dir] = the directions
+ * with no component along it; AXIS[dir] = its component index ({y,x} or
+ * {z,y,x}); SIGN[dir] = +1 or -1. */
+static const int REL9[5][3] = { {0,0,0}, {1,5,8}, {2,5,6}, {3,6,7}, {4,7,8} };
+static const int PERP9[5][3] = { {0,0,0}, {0,2,4}, {0,1,3}, {0,2,4}, {0,1,3} };
+static const int AXIS9[5] = {0, 1, 0, 1, 0};
+static const int SIGN9[5] = {0, 1, 1, -1, -1};
+static const int REL19[7][5] = { {0,0,0,0,0},
+    {1,7,9,11,13}, {2,8,10,12,14}, {3,8,7,15,17}, {4,9,10,16,18},
+    {5,11,12,15,16}, {6,13,14,17,18} };
+static const int PERP19[7][9] = { {0,0,0,0,0,0,0,0,0},
+    {0,3,4,5,6,15,16,17,18}, {0,3,4,5,6,15,16,17,18},
+    {0,1,2,5,6,11,12,13,14}, {0,1,2,5,6,11,12,13,14},
+    {0,1,2,3,4,7,8,9,10}, {0,1,2,3,4,7,8,9,10} };
+static const int AXIS19[7] = {0, 2, 2, 1, 1, 0, 0};
+static const int SIGN19[7] = {0, 1, -1, 1, -1, 1, -1};
+
 /* MRT transform matrices (solver/src/lbm/simulator.cpp:162-197). */
 static const double M9[81] = {
      1, 1, 1, 1, 1, 1, 1, 1, 1,
@@ -168,7 +187,11 @@ void lbo_mrt_tables(int q, double tau, double *m, double *minv, double *s)
     mrt_rates(q, tau, s);
 }
 
-static int is_fluid_type(int t) { return t == LBO_VD || t == LBO_GV; }
+/* Voxels that carry populations (the fluid sets of initialize, collision and
+ * buildIb: VD, GV, PB, VB; HF is a color research selector, refused). */
+static int is_fluid_type(int t) { return t == LBO_VD || t == LBO_GV || t == LBO_PB || t == LBO_VB; }
+/* Voxels whose moments come from the populations (calcMacroVar's VD, GV). */
+static int is_bulk_type(int t) { return t == LBO_VD || t == LBO_GV; }
 static int is_solid_type(int t) { return t == LBO_BB || t == LBO_SD; }
 
 /* Grid::calcAdjI (solver/inc/grid/grid.h:179-189): periodic neighbour. */
@@ -313,8 +336,14 @@ lbo_sim *lbo_create(const lbo_params *p, const lbo_label labels[256], const uint
     }
     s->phases = p->color ? 2 : 1;
     for (size_t i = 0; i < s->N; ++i) {
-        int t = labels[geometry[i]].type;
+        const lbo_label *l = &labels[geometry[i]];
+        int t = l->type;
         if (!is_fluid_type(t) && !is_solid_type(t)) { free(s); return NULL; }
+        /* FilePrm checks (fileprm.cpp:283-289); Zou-He is restated for SCSP only. */
+        if (t == LBO_PB || t == LBO_VB) {
+            if (p->color || l->dir < 1 || l->dir > 2 * s->D || !isfinite(l->value) ||
+                (t == LBO_PB && l->value <= 0.0)) { free(s); return NULL; }
+        }
     }
     s->geom = malloc(s->N);
     memcpy(s->geom, geometry, s->N);
@@ -412,7 +441,7 @@ static int scsp_macros(lbo_sim *s)
 {
     const double dens0 = s->p.rho[0];
     for (size_t i = 0; i < s->N; ++i) {
-        if (!is_fluid_type(s->lab[s->geom[i]].type)) continue;
+        if (!is_bulk_type(s->lab[s->geom[i]].type)) continue;
         double r = F(0, 0, i);
         for (int q = 1; q < s->Q; ++q) r += F(0, q, i);
         s->dens[0][i] = r;
@@ -484,6 +513,69 @@ static int scsp_collide(lbo_sim *s)
     for (size_t k = 0; k < (size_t)Q * s->N; ++k)
         if (!isfinite(s->f[k])) return LBO_ERR_NONFINITE;
     return LBO_OK;
+}
+
+/* SCSP::zouHeBoundary (scsp.cpp:188-275): velocity (VB) and pressure (PB)
+ * boundary voxels get their density and velocity from the known populations,
+ * then every unknown population (those along the boundary's direction) is
+ * rebuilt from its opposite.  wiT = 6 w / latticeSpeed (simulator.cpp:28),
+ * latticeSpeed = 1. */
+static void scsp_zou_he(lbo_sim *s)
+{
+    const int D = s->D;
+    for (size_t i = 0; i < s->N; ++i) {
+        const lbo_label *l = &s->lab[s->geom[i]];
+        if (l->type != LBO_PB && l->type != LBO_VB) continue;
+        const int dir = l->dir;
+        const int nrel = D == 2 ? 3 : 5, nperp = D == 2 ? 3 : 9;
+        const int opdir = s->op[dir];
+        const int *oprel = D == 2 ? REL9[opdir] : REL19[opdir];
+        const int *perp = D == 2 ? PERP9[dir] : PERP19[dir];
+        const int axis = D == 2 ? AXIS9[dir] : AXIS19[dir];
+        const int sign = D == 2 ? SIGN9[dir] : SIGN19[dir];
+        double sumF = 0;
+        for (int k = 0; k < nrel; ++k) sumF += F(0, oprel[k], i) + F(0, oprel[k], i);
+        for (int k = 0; k < nperp; ++k) sumF += F(0, perp[k], i);
+        if (l->type == LBO_VB) {
+            const double velocity = sign == 1 ? l->value : -l->value;
+            const double vel_1 = 1.0 / (1.0 - velocity);
+            for (int d = 0; d < D; ++d) s->v[d][i] = 0;
+            s->v[axis][i] = velocity;
+            s->dens[0][i] = sumF * vel_1;
+        } else {
+            const double density = l->value;
+            s->dens[0][i] = density;
+            for (int d = 0; d < D; ++d) s->v[d][i] = 0;
+            sumF /= density;
+            sumF--;
+            s->v[axis][i] = sign == 1 ? -sumF : sumF;
+        }
+    }
+    for (size_t i = 0; i < s->N; ++i) {
+        const lbo_label *l = &s->lab[s->geom[i]];
+        if (l->type != LBO_PB && l->type != LBO_VB) continue;
+        const int dir = l->dir;
+        const int nrel = D == 2 ? 3 : 5, nperp = D == 2 ? 3 : 9;
+        const int *rel = D == 2 ? REL9[dir] : REL19[dir];
+        const int *perp = D == 2 ? PERP9[dir] : PERP19[dir];
+        const int axis = D == 2 ? AXIS9[dir] : AXIS19[dir];
+        const int sign = D == 2 ? SIGN9[dir] : SIGN19[dir];
+        for (int k = 0; k < nrel; ++k) {
+            const int q = rel[k];
+            F(0, q, i) = F(0, s->op[q], i);
+            F(0, q, i) += sign * (6.0 * s->w[q]) * s->dens[0][i] * s->v[axis][i];
+            double sumF = 0;
+            for (int m = 0; m < nperp; ++m) {
+                const int qn = perp[m];
+                for (int d = 0; d < D; ++d) {
+                    if (s->e[qn][d] == 0 || s->e[q][d] == 0) continue;
+                    else if (s->e[qn][d] == s->e[q][d]) sumF += F(0, qn, i);
+                    else sumF -= F(0, qn, i);
+                }
+            }
+            F(0, q, i) -= sumF * 0.5;
+        }
+    }
 }
 
 /* ---- two-phase color gradient (ColorFluid) ----------------------------------- */
@@ -738,7 +830,9 @@ int lbo_stream_macros(lbo_sim *s)
 {
     if (!s) return LBO_ERR_ARG;
     stream_bounce(s);
-    return s->p.color ? color_macros(s) : scsp_macros(s);
+    if (s->p.color) return color_macros(s);
+    scsp_zou_he(s);
+    return scsp_macros(s);
 }
 
 int lbo_step(lbo_sim *s, int n)

@@ -24,8 +24,8 @@ enum { LBO_VD = 0x1, LBO_GV = 0x2, LBO_PB = 0x4, LBO_VB = 0x8,
 /* One geometry label (a line `N "TYPE" "value" "dir" "phase"` of input.prm). */
 typedef struct {
     int    type;   /* 0 = label not defined */
-    double value;  /* GV force magnitude or SD contact angle (degrees) */
-    int    dir;    /* GV lattice direction */
+    double value;  /* GV force magnitude, PB density, VB speed or SD contact angle (degrees) */
+    int    dir;    /* GV lattice direction; PB/VB boundary direction 1..2D */
     int    phase;  /* fluid phase (0 or 1) */
 } lbo_label;
 

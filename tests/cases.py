@@ -112,11 +112,63 @@ def porous_scsp_2d(collision='MRT'):
                 model='scsp', collision=collision, tau=(0.9,), rho=(1.0,), steps=400, write=400)
 
 
+def _boundary_channel(name, shape, axis, lo, hi, walls, collision, tau=(1.0,), wall_type='SD', steps=300):
+    """A channel along `axis` (0 = x, 1 = y, 2 = z) with Zou-He boundary planes:
+    `lo` / `hi` = (type, value, dir) on the first / last plane across the axis,
+    solid planes at both ends of the `walls` axis, VD inside."""
+    g = np.full(shape, 75, np.uint8)
+    nd = len(shape)
+
+    def sl(ax, i):
+        idx = [slice(None)] * nd
+        idx[nd - 1 - ax] = i
+        return tuple(idx)
+    g[sl(axis, 0)] = 50
+    g[sl(axis, -1)] = 200
+    g[sl(walls, 0)] = 255
+    g[sl(walls, -1)] = 255
+    labels = {75: ('VD', 0, 0, 0), 50: (lo[0], lo[1], lo[2], 0), 200: (hi[0], hi[1], hi[2], 0),
+              255: (wall_type, 90.0 if wall_type == 'SD' else 0.0, 0, 0)}
+    return dict(name=name, geometry=g, labels=labels, model='scsp', collision=collision, tau=tau,
+                rho=(1.0,), steps=steps, write=steps)
+
+
+def zou_he_cases():
+    """Pressure (PB) and velocity (VB) boundaries, SCSP::zouHeBoundary
+    (scsp.cpp:188-275), on every axis and both signs, D2Q9 and D3Q19, the
+    pressure channel of scripts/porous_media.py:257-279 in small, and a porous
+    medium whose inlet plane mixes PB voxels with bounce-back links."""
+    dp = 1 + 3 * 1e-4
+    out = [
+        _boundary_channel('pb-channel-d3-MRT', (3, 8, 17), 0, ('PB', dp, 1), ('PB', 1.0, 2), 1, 'MRT'),
+        _boundary_channel('pb-channel-d3-SRT', (3, 8, 17), 0, ('PB', dp, 1), ('PB', 1.0, 2), 1, 'SRT',
+                          tau=(0.8,)),
+        _boundary_channel('vb-channel-d3-MRT', (3, 8, 17), 0, ('VB', 1e-3, 1), ('PB', 1.0, 2), 1, 'MRT'),
+        _boundary_channel('vb-channel-y-d3-SRT', (3, 17, 8), 1, ('PB', 1.0, 3), ('VB', 1e-3, 4), 0, 'SRT',
+                          tau=(0.7,)),
+        _boundary_channel('pb-channel-z-d3-MRT', (17, 8, 4), 2, ('PB', dp, 5), ('PB', 1.0, 6), 1, 'MRT',
+                          tau=(1.3,)),
+        _boundary_channel('pb-channel-d2-MRT', (10, 24), 0, ('PB', dp, 1), ('PB', 1.0, 3), 1, 'MRT'),
+        _boundary_channel('vb-channel-y-d2-SRT', (24, 10), 1, ('PB', 1.0, 2), ('VB', 5e-4, 4), 0, 'SRT',
+                          tau=(0.9,), wall_type='BB'),
+    ]
+    c = porous_scsp('MRT')
+    g = c['geometry'].copy()
+    g[:, :, 0][g[:, :, 0] == 75] = 50
+    g[:, :, -1][g[:, :, -1] == 75] = 200
+    c.update(name='pb-porous-d3-MRT', geometry=g,
+             labels={75: ('VD', 0, 0, 0), 50: ('PB', dp, 1, 0), 200: ('PB', 1.0, 2, 0),
+                     255: ('SD', 90.0, 0, 0)})
+    out.append(c)
+    return out
+
+
 def golden_cases():
     """The cases whose reference outputs are committed under tests/golden/."""
     return ([channel_config1(), channel_mrt(), drop_3d(), wall_color_3d(0.7, 'MRT'),
              wall_color_3d(1.0, 'SRT'), wall_color_2d('MRT'), wall_color_2d('SRT'),
-             porous_scsp('MRT'), porous_scsp('SRT'), porous_scsp_2d('MRT')] + force_cases())
+             porous_scsp('MRT'), porous_scsp('SRT'), porous_scsp_2d('MRT')] + force_cases()
+            + zou_he_cases())
 
 
 def prm_text(case, grid_file='geometry.raw', out='field', report_dir=0):
@@ -145,9 +197,9 @@ def prm_text(case, grid_file='geometry.raw', out='field', report_dir=0):
         'wallGradient "legacy";', 'viscosityInterpolation "arithmetic";',
     ]
     for k, (t, v, d, ph) in sorted(case['labels'].items()):
-        val = 'N/A' if t in ('VD', 'BB') else format(v, '.17g') if t == 'GV' else format(v, 'g')
-        dr = str(d) if t == 'GV' else 'N/A'
-        p = str(ph) if t in ('VD', 'GV') else 'N/A'
+        val = 'N/A' if t in ('VD', 'BB') else format(v, '.17g') if t in ('GV', 'PB', 'VB') else format(v, 'g')
+        dr = str(d) if t in ('GV', 'PB', 'VB') else 'N/A'
+        p = str(ph) if t in ('VD', 'GV', 'PB', 'VB') else 'N/A'
         lines.append(f'{k} "{t}" "{val}" "{dr}" "{p}"')
     if not color:
         pass

@@ -8,7 +8,8 @@ final post-collision populations (the .rst checkpoint) and the last VTI fields
 as <case>.npz next to this script.  Run it in a checkout where oracle/_ref/
 exists; the tests only read the .npz files.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # every case + the CLI contracts
+    python tests/golden/make_golden.py NAME ...   # only the named cases
 """
 import json
 import subprocess
@@ -45,8 +46,11 @@ def main():
     exe = ROOT / 'oracle' / '_ref' / 'LBFlow'
     if not exe.exists():
         raise SystemExit('build the reference first: make -C oracle ref')
-    index = {}
+    only = set(sys.argv[1:])
+    index = json.loads((HERE / 'index.json').read_text()) if only else {}
     for case in golden_cases():
+        if only and case['name'] not in only:
+            continue
         with tempfile.TemporaryDirectory() as d:
             d = Path(d)
             case['geometry'].tofile(d / 'geometry.raw')
@@ -65,7 +69,8 @@ def main():
                                    total_voxels=timing['total_voxels'])
         print(case['name'], f.size, sorted(vti))
     (HERE / 'index.json').write_text(json.dumps(index, indent=1, sort_keys=True) + '\n')
-    cli_contracts(exe)
+    if not only:
+        cli_contracts(exe)
 
 
 def run_ref(exe, case, prm=None, extra=None):
