@@ -77,10 +77,14 @@ enum {
  * after FilePrm::IDXVAL parsing (solver/src/file/fileprm.cpp:633-670). */
 typedef struct {
     int32_t type;     /* LBF_VD ... LBF_SD; 0 = label not defined */
-    int32_t dir;      /* GV: lattice direction of the force */
-    int32_t phase;    /* VD/GV: fluid phase */
+    int32_t dir;      /* GV: lattice direction of the force; PB/VB: the axial
+                         direction 1..2*dims pointing into the domain (the
+                         direction of the populations the boundary rebuilds) */
+    int32_t phase;    /* VD/GV/PB/VB: fluid phase */
     int32_t reserved;
-    double value;     /* GV: force magnitude; SD: contact angle in degrees */
+    double value;     /* GV: force magnitude; PB: density; VB: speed along dir
+                         (SCSP::zouHeBoundary, scsp.cpp:188-275; single phase
+                         only); SD: contact angle in degrees */
 } lbf_label;
 
 typedef struct {

@@ -42,6 +42,9 @@ struct lbf_engine {
     double* h_red = nullptr;        // pinned
     cudaStream_t stream = nullptr;
     Force force{};
+    ZouHe zh{};                     // PB/VB boundary nodes (single phase)
+    uint32_t *zh_node = nullptr, *zh_code = nullptr;
+    double* zh_value = nullptr;
     ScspParams sp{};
     ColorParams cp{};
     bool initialized = false;
@@ -87,7 +90,10 @@ const int kE19[19][3] = {{0,0,0},{0,0,1},{0,0,-1},{0,1,0},{0,-1,0},{1,0,0},{-1,0
     {0,1,1},{0,1,-1},{0,-1,1},{0,-1,-1},{1,0,1},{1,0,-1},{-1,0,1},{-1,0,-1},
     {1,1,0},{1,-1,0},{-1,1,0},{-1,-1,0}};
 
-bool is_fluid(int t) { return t == LBF_VD || t == LBF_GV; }
+// Voxels that carry populations: the fluid sets of SCSP::initialize /
+// collision and Simulator::buildIb (scsp.cpp:116-134, 374-464;
+// simulator.cpp:399-415).  PB/VB are accepted for the single-phase model only.
+bool is_fluid(int t) { return t == LBF_VD || t == LBF_GV || t == LBF_PB || t == LBF_VB; }
 bool is_solid(int t) { return t == LBF_BB || t == LBF_SD; }
 
 // e_q component a (0 = x, 1 = y, 2 = z) of the reference tables.
@@ -168,8 +174,11 @@ void launch_step(lbf_engine* e, bool pull, int out)
     void* fout = e->f[e->cur ^ 1];
     if (e->cfg.model == LBF_MODEL_SCSP) {
         ScspLaunch a{grid_of(e), e->force, e->sp, fin, fout, macros_of(e), e->err, e->stream,
-                     e->ex[e->cur], e->ex[e->cur ^ 1]};
+                     e->ex[e->cur], e->ex[e->cur ^ 1], out};
         launch_scsp(e->D, (int)e->cfg.storage, e->cfg.collision == LBF_MRT, pull, out, a);
+        // At t = 0 (no pull) the boundary nodes hold rho0 at rest, which the
+        // main kernel reproduces from their initial populations.
+        if (pull && e->zh.n) launch_scsp_zou_he(e->D, (int)e->cfg.storage, a, e->zh);
     } else {
         ColorWall W{e->angle_id, e->angles, e->tib};
         ColorLaunch a{grid_of(e), e->force, e->cp, W, fin, fout, e->phi, macros_of(e), e->err, e->stream};
@@ -390,7 +399,18 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
         const lbf_label& L = labels[l];
         if (L.type == 0) return bail(LBF_EINVAL, "geometry label " + std::to_string(l) + " is not defined");
         if (!is_fluid(L.type) && !is_solid(L.type))
-            return bail(LBF_EINVAL, "label " + std::to_string(l) + ": only VD, GV, BB and SD labels are supported");
+            return bail(LBF_EINVAL, "label " + std::to_string(l) + ": only VD, GV, PB, VB, BB and SD labels are supported");
+        if ((L.type == LBF_PB || L.type == LBF_VB) && c.model != LBF_MODEL_SCSP)
+            return bail(LBF_EINVAL, "label " + std::to_string(l) +
+                                        ": PB/VB boundaries are supported for the single-phase model only");
+        if ((L.type == LBF_PB || L.type == LBF_VB) && !std::isfinite(L.value))
+            return bail(LBF_EINVAL, "Non-finite boundary value.");
+        if ((L.type == LBF_PB || L.type == LBF_VB) && (L.dir <= 0 || L.dir >= e->Q))
+            return bail(LBF_EINVAL, "Boundary direction must be a non-rest lattice direction.");
+        if (L.type == LBF_PB && L.value <= 0.0)
+            return bail(LBF_EINVAL, "Pressure-boundary density must be positive.");
+        if ((L.type == LBF_PB || L.type == LBF_VB) && L.dir > 2 * e->D)
+            return bail(LBF_EINVAL, "Pressure and velocity boundaries require an axial direction.");
         if (is_fluid(L.type) && (L.phase < 0 || L.phase >= phases))
             return bail(LBF_EINVAL, "Boundary phase is outside the configured fluid model.");
         if (L.type == LBF_GV && (L.dir <= 0 || L.dir >= e->Q || !std::isfinite(L.value)))
@@ -434,6 +454,17 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
             nphase[k] = (uint8_t)labels[l].phase;
             ++k;
         }
+    }
+
+    // Zou-He boundary nodes in compact order (SCSP::zouHeBoundary, scsp.cpp:188-275).
+    std::vector<uint32_t> zh_node, zh_code;
+    std::vector<double> zh_value;
+    for (uint32_t k = 0; k < e->nf; ++k) {
+        const lbf_label& L = labels[nlabel[k]];
+        if (L.type != LBF_PB && L.type != LBF_VB) continue;
+        zh_node.push_back(k);
+        zh_code.push_back(((L.type == LBF_VB ? kZouHeVB : kZouHePB) << 8) | (uint32_t)L.dir);
+        zh_value.push_back(L.value);
     }
 
     // Body force per label, x/y/z (Simulator::forceForIndex, simulator.cpp:218-228:
@@ -489,6 +520,18 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
     LBF_CUDA(cudaMemcpyAsync(e->occ, occ.data(), occ.size() * sizeof(uint2), cudaMemcpyHostToDevice, e->stream));
     LBF_CUDA(cudaMemcpyAsync(e->coord, coord.data(), coord.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, e->stream));
     LBF_CUDA(cudaMemcpyAsync(e->label_force, lforce.data(), lforce.size() * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+    if (!zh_node.empty()) {
+        LBF_ALLOC(e->zh_node, zh_node.size());
+        LBF_ALLOC(e->zh_code, zh_code.size());
+        LBF_ALLOC(e->zh_value, zh_value.size());
+        LBF_CUDA(cudaMemcpyAsync(e->zh_node, zh_node.data(), zh_node.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, e->stream));
+        LBF_CUDA(cudaMemcpyAsync(e->zh_code, zh_code.data(), zh_code.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, e->stream));
+        LBF_CUDA(cudaMemcpyAsync(e->zh_value, zh_value.data(), zh_value.size() * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+        e->zh.n = (uint32_t)zh_node.size();
+        e->zh.node = e->zh_node;
+        e->zh.code = e->zh_code;
+        e->zh.value = e->zh_value;
+    }
     if (!uniform) {
         LBF_ALLOC(e->node_label, e->nfp);
         LBF_CUDA(cudaMemcpyAsync(e->node_label, nlabel.data(), nlabel.size(), cudaMemcpyHostToDevice, e->stream));
@@ -516,6 +559,7 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
         e->sp.rho0 = c.rho[0];
         e->sp.inv_rho0 = 1.0 / c.rho[0];
         e->sp.rate = rates(c.collision == LBF_MRT, c.tau[0]);
+        e->sp.mrt = c.collision == LBF_MRT ? 1 : 0;
     } else {
         // ColorFluid::initPhi (colorfluid.cpp:1131-1150).
         double alpha[2];
@@ -621,7 +665,8 @@ void lbf_destroy(lbf_engine* e)
     if (e->stream) cudaStreamSynchronize(e->stream);
     void* ptrs[] = {e->f[0], e->f[1], e->ex[0], e->ex[1], e->occ, e->coord, e->node_label, e->node_phase, e->label_force,
                     e->rho0, e->rho1, e->u, e->uprev, e->uadj, e->ind, e->indprev, e->indadj,
-                    e->phi, e->angle_id, e->angles, e->tib, e->err, e->partial, e->red};
+                    e->phi, e->angle_id, e->angles, e->tib, e->err, e->partial, e->red,
+                    e->zh_node, e->zh_code, e->zh_value};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (e->h_red) cudaFreeHost(e->h_red);
     if (e->stream) cudaStreamDestroy(e->stream);

@@ -19,6 +19,7 @@ struct ScspLaunch {
     cudaStream_t stream;
     const int8_t* ein;   // block exponents of fin (block-scaled storage only)
     int8_t* eout;
+    int out;             // kOutMacros / kOutAdjacent of this step (boundary pass)
 };
 
 struct ColorLaunch {
@@ -38,6 +39,8 @@ struct ColorLaunch {
 void launch_scsp(int dims, int storage, bool mrt, bool pull, int out, const ScspLaunch& a);
 void launch_scsp_init(int dims, int storage, const Grid& g, const Force& F, double rho0,
                       void* f, int8_t* eout, cudaStream_t s);
+// Zou-He PB/VB boundary pass of one pull step (after launch_scsp, same buffers).
+void launch_scsp_zou_he(int dims, int storage, const ScspLaunch& a, const ZouHe& z);
 void launch_scsp_add_density(int dims, int storage, const Grid& g, const float* drho, void* f, int8_t* eio,
                              double rho0, cudaStream_t s);
 void launch_scsp_init_eq(int dims, int storage, const Grid& g, const Force& F, double rho0, const float* fields,

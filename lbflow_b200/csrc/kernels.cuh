@@ -316,6 +316,7 @@ struct ScspParams {
     double rho0;       // reference density (incompressible form, lbcfg.h:13)
     double inv_rho0;
     Trt rate;          // SRT: s+ = s- = 1/tau; MRT: legacy spectrum
+    int mrt = 0;       // MRT: mass and momentum rows are not relaxed (rate 0)
 };
 
 // Update of one fluid node i (the body of scsp_step, shared with the batched
@@ -398,6 +399,189 @@ scsp_step(const Grid g, const Force F, const ScspParams P,
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= g.nf) return;
     scsp_update<L, S, PULL>(g, F, P, fin, fout, i, mo, out, err, ein, eout);
+}
+
+// ---- Zou-He pressure (PB) and velocity (VB) boundaries ---------------------------
+// SCSP::zouHeBoundary (scsp.cpp:188-275) runs between streaming and the
+// macroscopic update; PB/VB voxels then skip calcMacroVar (scsp.cpp:136-160)
+// and collide with the density and velocity it set, under zero force
+// (forceForIndex is zero for non-GV labels, simulator.cpp:218-228).  The main
+// step kernel treats every fluid node alike; this pass, launched right after
+// it on the same stream, recomputes the boundary nodes from the same input
+// buffer and overwrites their populations and fields.
+struct ZouHe {
+    uint32_t n;                          // boundary nodes
+    const uint32_t* __restrict__ node;   // compact node index
+    const uint32_t* __restrict__ code;   // kind << 8 | dir (dir 1..2D, the lattice direction)
+    const double* __restrict__ value;    // PB density or VB speed
+};
+enum : uint32_t { kZouHeVB = 1, kZouHePB = 2 };
+
+// Axis (0 = x, 1 = y, 2 = z) and sign of the axial lattice direction DIR.
+template <class L, int DIR> struct ZouHeDir {
+    static constexpr int A = L::ex(DIR) != 0 ? 0 : (L::ey(DIR) != 0 ? 1 : 2);
+    static constexpr int SG = comp<L>(DIR, A);
+};
+
+// Density and velocity of the boundary node from the known populations, then
+// the unknown populations (those with the boundary direction's sign along its
+// axis) rebuilt from their opposites:
+//   VB: u_a = s v, rho = (2 sum f[opposite side] + sum f[normal plane]) / (1 - u_a)
+//   PB: rho = p,   u_a = -s (that sum / p - 1)
+//   f_q = f_op(q) + s 6 w_q rho u_a - 1/2 sum_{n in plane} (+-) f_n
+// (6 w_q = wiT of simulator.cpp:28 at latticeSpeed 1)
+// where the last sum runs over the normal-plane directions sharing a
+// transverse component with q, + when the components agree.  With shifted
+// storage (f - w rho0) the sums are rewritten so that only deviations are
+// formed: the plane and opposite-side weights add up to 1 and the transverse
+// sum is unchanged because mirrored directions have equal weights.
+// Returns rho (a deviation when shifted) and the full density in dens.
+template <class L, class S, int DIR>
+__device__ __forceinline__ typename S::R zou_he_node(typename S::R (&f)[L::Q], uint32_t kind, double val,
+                                                     double rho0, typename S::R (&u)[3], double& dens)
+{
+    using R = typename S::R;
+    constexpr int A = ZouHeDir<L, DIR>::A, SG = ZouHeDir<L, DIR>::SG;
+    R sum = R(0);
+#pragma unroll
+    for (int q = 1; q < L::Q; ++q)
+        if (comp<L>(q, A) == -SG) sum += f[q] + f[q];
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q)
+        if (comp<L>(q, A) == 0) sum += f[q];
+    R rho, ua;
+    if (kind == kZouHeVB) {
+        const double vel = SG > 0 ? val : -val;
+        const R inv = R(1.0 / (1.0 - vel));
+        ua = R(vel);
+        if constexpr (S::shifted) { rho = (sum + R(rho0 * vel)) * inv; dens = rho0 + (double)rho; }
+        else { rho = sum * inv; dens = (double)rho; }
+    } else {
+        R s;
+        if constexpr (S::shifted) { rho = R(val - rho0); s = (sum - rho) / R(val); }
+        else { rho = R(val); s = sum / R(val) - R(1); }
+        ua = SG > 0 ? -s : s;
+        dens = val;
+    }
+    const R rho_full = R(dens);
+    R tr[L::Q];
+#pragma unroll
+    for (int q = 1; q < L::Q; ++q) {
+        if (comp<L>(q, A) != SG) continue;
+        R t = R(0);
+#pragma unroll
+        for (int n = 1; n < L::Q; ++n) {
+            if (comp<L>(n, A) != 0) continue;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                if (d == A || comp<L>(n, d) == 0 || comp<L>(q, d) == 0) continue;
+                if (comp<L>(n, d) == comp<L>(q, d)) t += f[n];
+                else t -= f[n];
+            }
+        }
+        tr[q] = t;
+    }
+#pragma unroll
+    for (int q = 1; q < L::Q; ++q) {
+        if (comp<L>(q, A) != SG) continue;
+        f[q] = f[L::op(q)] + R(SG) * R(6.0 * w<L>(q)) * rho_full * ua - tr[q] * R(0.5);
+    }
+    u[0] = u[1] = u[2] = R(0);
+    u[A] = ua;
+    return rho;
+}
+
+template <class L, class S>
+__global__ void __launch_bounds__(128)
+scsp_zou_he(const Grid g, const ScspParams P, const ZouHe z,
+            const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
+            Macros mo, const int out, uint32_t* __restrict__ err,
+            const int8_t* __restrict__ ein, int8_t* __restrict__ eout)
+{
+    using R = typename S::R;
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= z.n) return;
+    const uint32_t i = __ldg(&z.node[k]);
+    const uint32_t code = __ldg(&z.code[k]);
+    const double val = __ldg(&z.value[k]);
+    int x, y, zc;
+    unpack(__ldg(&g.coord[i]), x, y, zc);
+    const R rho0 = R(P.rho0);
+    R f[L::Q];
+    uint32_t nbr[L::Q];
+    gather<L, S, true>(g, fin, i, x, y, zc, f, nbr, rho0, ein);
+
+    const uint32_t kind = code >> 8;
+    R u[3];
+    R rho = R(0);
+    double dens = 0.0;
+    switch (code & 0xffu) {
+    case 1: rho = zou_he_node<L, S, 1>(f, kind, val, P.rho0, u, dens); break;
+    case 2: rho = zou_he_node<L, S, 2>(f, kind, val, P.rho0, u, dens); break;
+    case 3: rho = zou_he_node<L, S, 3>(f, kind, val, P.rho0, u, dens); break;
+    case 4: rho = zou_he_node<L, S, 4>(f, kind, val, P.rho0, u, dens); break;
+    default:
+        if constexpr (L::D == 3) {
+            if ((code & 0xffu) == 5) rho = zou_he_node<L, S, 5>(f, kind, val, P.rho0, u, dens);
+            else rho = zou_he_node<L, S, 6>(f, kind, val, P.rho0, u, dens);
+        }
+        break;
+    }
+    if (!isfinite(dens) || !isfinite((double)u[0] + (double)u[1] + (double)u[2])) atomicOr(err, kErrDensity);
+
+    if (out & (kOutMacros | kOutAdjacent)) {
+        // The reference takes the adjacent-step copy after zouHeBoundary of the
+        // report step (scsp.cpp:80-81), so at these nodes it equals the reported
+        // velocity.
+#pragma unroll
+        for (int a = 0; a < 3; ++a) mo.uadj[(size_t)a * g.nfp + i] = (double)u[a];
+    }
+    if (out & kOutMacros) {
+        mo.rho0[i] = dens;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) mo.u[(size_t)a * g.nfp + i] = (double)u[a];
+    }
+
+    // The two-rate update relaxes the mass row at s+ and the momentum rows at
+    // s-, whereas the reference's MRT leaves them untouched (rate 0,
+    // simulator.cpp:209-214).  In the bulk the difference vanishes (feq - f
+    // carries no mass and only the momentum the Guo term restores), but here
+    // the populations' mass and momentum differ from the prescribed rho and
+    // rho0 u, so those two projections of feq - f are taken back out:
+    // M^-1 diag(s) M d over the conserved rows is s (sum d) / Q on every
+    // direction and s e_q . J / |e_a|^2 with J = sum e d.
+    R dmass = R(0), dmom[3] = {R(0), R(0), R(0)};
+    if (P.mrt) {
+        R sf = f[0];
+#pragma unroll
+        for (int q = 1; q < L::Q; ++q) sf += f[q];
+#pragma unroll
+        for (int q = 1; q < L::Q; ++q) {
+            if (L::ex(q)) dmom[0] -= R(L::ex(q)) * f[q];
+            if (L::ey(q)) dmom[1] -= R(L::ey(q)) * f[q];
+            if (L::ez(q)) dmom[2] -= R(L::ez(q)) * f[q];
+        }
+        dmass = rho - sf;               // sum of feq is rho (a deviation when shifted)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) dmom[a] += rho0 * u[a];   // sum of e feq is rho0 u
+    }
+    const R usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    const R F0[3] = {R(0), R(0), R(0)};
+    collide_trt<L, R, false>(f, nullptr, rho - rho0 * R(1.5) * usq, rho0 * R(4.5), rho0 * R(3),
+                             u, F0, R(0), R(P.rate.sp), R(P.rate.sm));
+    if (P.mrt) {
+        const R cm = R(P.rate.sp) * dmass / R(L::Q);
+        const R cj = R(P.rate.sm) / R(L::D == 3 ? 10 : 6);   // |e_a|^2 over the velocity set
+#pragma unroll
+        for (int q = 0; q < L::Q; ++q)
+            f[q] -= cm + cj * (R(L::ex(q)) * dmom[0] + R(L::ey(q)) * dmom[1] + R(L::ez(q)) * dmom[2]);
+    }
+    if constexpr (S::blocked) {
+        S::store_blk(fout, g.nfp, i, f, eout);
+    } else {
+#pragma unroll
+        for (int q = 0; q < L::Q; ++q) S::store(fout + (q * g.nfp + i), f[q], q, rho0);
+    }
 }
 
 // t = 0 populations of SCSP::initialize (scsp.cpp:116-134):

@@ -32,6 +32,29 @@ void dispatch_storage(int storage, bool mrt, bool pull, int out, const ScspLaunc
     }
 }
 
+template <class L, class S>
+void zou_he(const ScspLaunch& a, const ZouHe& z)
+{
+    using T = typename S::T;
+    const unsigned threads = 128, blocks = blocks_for(z.n, threads);
+    if (blocks == 0) return;
+    scsp_zou_he<L, S><<<blocks, threads, 0, a.stream>>>(a.g, a.P, z, static_cast<const T*>(a.fin),
+                                                         static_cast<T*>(a.fout), a.mo, a.out, a.err,
+                                                         a.ein, a.eout);
+}
+
+template <class L>
+void zou_he_storage(int storage, const ScspLaunch& a, const ZouHe& z)
+{
+    switch (storage) {
+    case LBF_STORE_FP64: zou_he<L, StoreF64>(a, z); break;
+    case LBF_STORE_FP16: zou_he<L, StoreF16<L>>(a, z); break;
+    case LBF_STORE_BF16: zou_he<L, StoreBF16<L>>(a, z); break;
+    case LBF_STORE_BFP16: zou_he<L, StoreBFP16<L>>(a, z); break;
+    default: zou_he<L, StoreF32<L>>(a, z); break;
+    }
+}
+
 template <class L>
 void init_storage(int storage, const Grid& g, const Force& F, double rho0, void* f, int8_t* e, cudaStream_t s)
 {
@@ -93,6 +116,12 @@ void launch_scsp(int dims, int storage, bool mrt, bool pull, int out, const Scsp
 {
     if (dims == 3) dispatch_storage<D3Q19>(storage, mrt, pull, out, a);
     else dispatch_storage<D2Q9>(storage, mrt, pull, out, a);
+}
+
+void launch_scsp_zou_he(int dims, int storage, const ScspLaunch& a, const ZouHe& z)
+{
+    if (dims == 3) zou_he_storage<D3Q19>(storage, a, z);
+    else zou_he_storage<D2Q9>(storage, a, z);
 }
 
 void launch_scsp_init(int dims, int storage, const Grid& g, const Force& F, double rho0,

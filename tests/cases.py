@@ -163,6 +163,25 @@ def zou_he_cases():
     return out
 
 
+def pressure_report_channel():
+    """scripts/porous_media.py:257-279 (pressure_study): a 16-wide slit between
+    SD walls, PB inlet 1 + 3e-5 and outlet 1 along x, MRT tau 1, 6000 steps,
+    reports every 2000 steps, latticeLen 1e-6 so that K is in lattice units.
+    The reference accepts it when the reported pressure drop and K are within
+    2e-4 of dp (nx - 3) / (nx - 1) and (h^3/12 + h/24) / (h + 2)."""
+    h, nx, nz, dp = 16, 65, 4, 1e-5
+    g = np.full((nz, h + 2, nx), 75, np.uint8)
+    g[:, :, 0] = 50
+    g[:, :, -1] = 200
+    g[:, 0, :] = 255
+    g[:, -1, :] = 255
+    return dict(name='pressure-channel-report', geometry=g,
+                labels={50: ('PB', 1 + 3 * dp, 1, 0), 200: ('PB', 1.0, 2, 0), 75: ('VD', 0, 0, 0),
+                        255: ('SD', 90.0, 0, 0)},
+                model='scsp', collision='MRT', tau=(1.0,), rho=(1.0,), steps=6000, write=2000,
+                stop_error=1e-12, lattice_len=1e-6, h=h, dp=dp)
+
+
 def golden_cases():
     """The cases whose reference outputs are committed under tests/golden/."""
     return ([channel_config1(), channel_mrt(), drop_3d(), wall_color_3d(0.7, 'MRT'),
@@ -184,7 +203,7 @@ def prm_text(case, grid_file='geometry.raw', out='field', report_dir=0):
     color = case['model'] == 'color'
     lines = [
         f'gridFile "{grid_file}";', f'dimension {dims};', f'directions {9 if ndim == 2 else 19};',
-        'fileType "uint8";', 'latticeLen 1;', 'startTime 0;', f'endTime {case["steps"]};',
+        'fileType "uint8";', f'latticeLen {case.get("lattice_len", 1)};', 'startTime 0;', f'endTime {case["steps"]};',
         f'writeInterval {case["write"]};', f'reportInterval {case.get("report", case["write"])};',
         f'restartInterval {case.get("restart", case["steps"])};',
         f'stopError {case.get("stop_error", 1e-8)};', f'outPath "{out}";', 'logPath ".";',

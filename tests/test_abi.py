@@ -45,7 +45,12 @@ def _create(**over):
     (dict(collision=5), 'collision'),
     (dict(tau=(0.5, 1.0)), 'relaxation times must exceed 0.5'),
     (dict(labels={}), 'not defined'),
-    (dict(labels={0: ('PB', 1.0, 1, 0)}), 'only VD, GV, BB and SD'),
+    (dict(labels={0: ('HF', 0.0, 0, 0)}), 'only VD, GV, PB, VB, BB and SD'),
+    (dict(model=1, labels={0: ('PB', 1.0, 1, 0)}), 'single-phase model only'),
+    (dict(labels={0: ('PB', 0.0, 1, 0)}), 'Pressure-boundary density must be positive'),
+    (dict(labels={0: ('VB', 1e-3, 7, 0)}), 'axial direction'),
+    (dict(labels={0: ('VB', 1e-3, 0, 0)}), 'non-rest lattice direction'),
+    (dict(labels={0: ('VB', float('nan'), 1, 0)}), 'Non-finite boundary value'),
     (dict(labels={0: ('GV', 1e-6, 19, 0)}), 'body-force direction'),
     (dict(labels={0: ('VD', 0, 0, 1)}), 'phase'),
     (dict(model=1, storage=1), 'two-phase storage'),

@@ -16,7 +16,8 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from cases import channel_mrt, drop_3d, golden_cases, porous_scsp, prm_text, wall_color_2d, wall_color_3d
+from cases import (channel_mrt, drop_3d, force_cases, golden_cases, porous_scsp, pressure_report_channel, prm_text,
+                   wall_color_2d, wall_color_3d)
 from conftest import GOLDEN, fluid_mask, load_golden
 
 ROOT = Path(__file__).resolve().parent.parent
@@ -81,9 +82,11 @@ def test_unsupported_options_are_refused(tmp_path):
         text = prm_text(case).replace('wallGradient "legacy";', f'{key} {val};')
         code, out = run_cli(tmp_path / key, case, text)
         assert code != 0 and 'not supported by the B200 engine' in out
-    text = prm_text(case).replace('75 "GV" "9.9999999999999995e-07" "1" "0"', '75 "PB" "1.0" "1" "0"')
-    code, out = run_cli(tmp_path / 'pb', case, text)
-    assert code != 0 and 'PB/VB' in out
+    color = force_cases()[-1]
+    text = prm_text(color).replace('75 "GV" "9.9999999999999995e-07" "1" "1"', '75 "PB" "1.0" "1" "1"')
+    assert '"PB"' in text
+    code, out = run_cli(tmp_path / 'pb', color, text)
+    assert code != 0 and 'PB/VB' in out and 'single-phase' in out
 
 
 # ---- GPU runs -----------------------------------------------------------------
@@ -136,7 +139,7 @@ def _numbers(line):
 @pytest.mark.parametrize('name', sorted(CONTRACTS['reports']))
 def test_report_lines_match_reference(tmp_path, name):
     spec = CONTRACTS['reports'][name]
-    base = porous_scsp('MRT') if name.startswith('porous') else wall_color_3d(0.7, 'MRT')
+    base = {c['name']: c for c in golden_cases() + [pressure_report_channel()]}[name]
     case = dict(base, report=spec['report'], steps=spec['steps'])
     code, out = run_cli(tmp_path, case, prm_text(case, report_dir=spec['report_dir']))
     assert code == 0, out[-2000:]
@@ -150,6 +153,21 @@ def test_report_lines_match_reference(tmp_path, name):
         assert re.sub(r'[-+]?\d+\.\d+(e[-+]\d+)?', '#', got) == re.sub(r'[-+]?\d+\.\d+(e[-+]\d+)?', '#', ref)
         for a, b in zip(_numbers(got), _numbers(ref)):
             assert math.isclose(a, b, rel_tol=2e-5, abs_tol=2e-6), (got, ref)
+
+
+@pytest.mark.gpu
+def test_pressure_study_acceptance(tmp_path):
+    """scripts/porous_media.py:257-279: the pressure-driven slit reports the
+    prescribed pressure drop between its report slices and the analytic slit
+    permeability, each within 2e-4."""
+    case = pressure_report_channel()
+    code, out = run_cli(tmp_path, case, prm_text(case, report_dir=1))
+    assert code == 0, out[-2000:]
+    dp = float(re.findall(r' - dP = ([\deE+.-]+)', out)[-1])
+    k = float(re.findall(r' - K = ([\deE+.-]+)', out)[-1])
+    h, nx = case['h'], case['geometry'].shape[2]
+    assert abs(dp / (case['dp'] * (nx - 3) / (nx - 1)) - 1) <= 2e-4
+    assert abs(k / ((h ** 3 / 12 + h / 24) / (h + 2)) - 1) <= 2e-4
 
 
 @pytest.mark.gpu
