@@ -339,10 +339,12 @@ lbo_sim *lbo_create(const lbo_params *p, const lbo_label labels[256], const uint
         const lbo_label *l = &labels[geometry[i]];
         int t = l->type;
         if (!is_fluid_type(t) && !is_solid_type(t)) { free(s); return NULL; }
-        /* FilePrm checks (fileprm.cpp:283-289); Zou-He is restated for SCSP only. */
+        /* FilePrm checks (fileprm.cpp:280-289). */
         if (t == LBO_PB || t == LBO_VB) {
-            if (p->color || l->dir < 1 || l->dir > 2 * s->D || !isfinite(l->value) ||
-                (t == LBO_PB && l->value <= 0.0)) { free(s); return NULL; }
+            if (l->dir < 1 || l->dir > 2 * s->D || !isfinite(l->value) ||
+                (t == LBO_PB && l->value <= 0.0) || l->phase < 0 || l->phase > (p->color ? 1 : 0)) {
+                free(s); return NULL;
+            }
         }
     }
     s->geom = malloc(s->N);
@@ -579,6 +581,71 @@ static void scsp_zou_he(lbo_sim *s)
 }
 
 /* ---- two-phase color gradient (ColorFluid) ----------------------------------- */
+/* ColorFluid::zouHeBoundary (colorfluid.cpp:638-734): the single-phase rule
+ * applied to the total distribution f0 + f1; the rebuilt unknowns go to the
+ * label's phase and the other phase's unknowns are cleared.  The density and
+ * velocity it sets are intermediates: calcMacroVar recomputes them from the
+ * populations (PB/VB are in its node set). */
+static void color_zou_he(lbo_sim *s)
+{
+    const int D = s->D;
+    for (size_t i = 0; i < s->N; ++i) {
+        const lbo_label *l = &s->lab[s->geom[i]];
+        if (l->type != LBO_PB && l->type != LBO_VB) continue;
+        const int dir = l->dir;
+        const int nrel = D == 2 ? 3 : 5, nperp = D == 2 ? 3 : 9;
+        const int *oprel = D == 2 ? REL9[s->op[dir]] : REL19[s->op[dir]];
+        const int *perp = D == 2 ? PERP9[dir] : PERP19[dir];
+        const int axis = D == 2 ? AXIS9[dir] : AXIS19[dir];
+        const int sign = D == 2 ? SIGN9[dir] : SIGN19[dir];
+        double sumF = 0;
+        for (int k = 0; k < nrel; ++k)
+            sumF += F(0, oprel[k], i) + F(0, oprel[k], i) + F(1, oprel[k], i) + F(1, oprel[k], i);
+        for (int k = 0; k < nperp; ++k) sumF += F(0, perp[k], i) + F(1, perp[k], i);
+        for (int d = 0; d < D; ++d) s->v[d][i] = 0;
+        if (l->type == LBO_VB) {
+            const double velocity = sign == 1 ? l->value : -l->value;
+            const double vel_1 = 1.0 / (1.0 - velocity);
+            s->v[axis][i] = velocity;
+            s->densT[i] = sumF * vel_1;
+        } else {
+            const double density = l->value;
+            s->densT[i] = density;
+            sumF /= density;
+            sumF--;
+            s->v[axis][i] = sign == 1 ? -sumF : sumF;
+        }
+    }
+    for (size_t i = 0; i < s->N; ++i) {
+        const lbo_label *l = &s->lab[s->geom[i]];
+        if (l->type != LBO_PB && l->type != LBO_VB) continue;
+        const int dir = l->dir;
+        const int nrel = D == 2 ? 3 : 5, nperp = D == 2 ? 3 : 9;
+        const int *rel = D == 2 ? REL9[dir] : REL19[dir];
+        const int *perp = D == 2 ? PERP9[dir] : PERP19[dir];
+        const int axis = D == 2 ? AXIS9[dir] : AXIS19[dir];
+        const int sign = D == 2 ? SIGN9[dir] : SIGN19[dir];
+        const int phs = l->phase, phsOp = 1 - phs;
+        for (int k = 0; k < nrel; ++k) {
+            const int q = rel[k];
+            double fT = F(0, s->op[q], i) + F(1, s->op[q], i);
+            fT += sign * (6.0 * s->w[q]) * s->densT[i] * s->v[axis][i];
+            double sumF = 0;
+            for (int m = 0; m < nperp; ++m) {
+                const int qn = perp[m];
+                for (int d = 0; d < D; ++d) {
+                    if (s->e[qn][d] == 0 || s->e[q][d] == 0) continue;
+                    else if (s->e[qn][d] == s->e[q][d]) sumF += F(0, qn, i) + F(1, qn, i);
+                    else sumF -= F(0, qn, i) + F(1, qn, i);
+                }
+            }
+            fT -= sumF * 0.5;
+            F(phs, q, i) = fT;
+            F(phsOp, q, i) = 0;
+        }
+    }
+}
+
 /* ColorFluid::initialize (colorfluid.cpp:214-236). */
 static void color_initialize(lbo_sim *s)
 {
@@ -830,7 +897,10 @@ int lbo_stream_macros(lbo_sim *s)
 {
     if (!s) return LBO_ERR_ARG;
     stream_bounce(s);
-    if (s->p.color) return color_macros(s);
+    if (s->p.color) {
+        color_zou_he(s);
+        return color_macros(s);
+    }
     scsp_zou_he(s);
     return scsp_macros(s);
 }

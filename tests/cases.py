@@ -163,6 +163,69 @@ def zou_he_cases():
     return out
 
 
+def entry_case(ratio=1.5, ndim=2, h=16, nx=None, steps=8000, write=2000, collision='MRT', tau=(1.0, 1.0)):
+    """The capillary-entry slit of scripts/porous_media.py:154-182 (entry_cases,
+    legacy walls): phase 0 fills x < h and is pushed by a PB inlet (density
+    1 + 3 dp, phase 0, direction +x) into a slit of phase 1 held by a PB outlet
+    (density 1, phase 1, direction -x); SD walls at 60 degrees; dp = ratio
+    times the sharp entry pressure 2 sigma cos 60 / h (4 sigma ... in 3D)."""
+    import math
+    nx = nx or 4 * h + 1
+    sigma = 0.005 * 16 / h if h != 16 else 0.005
+    pc = (2 if ndim == 2 else 4) * sigma * math.cos(math.radians(60)) / h
+    dp = ratio * pc
+    shape = (h + 2, nx) if ndim == 2 else (h + 2, h + 2, nx)
+    g = np.full(shape, 100, np.uint8)
+    xs = np.arange(nx)
+    g[..., xs < h] = 0
+    g[..., 0] = 50
+    g[..., -1] = 200
+    if ndim == 2:
+        g[0, :] = 255
+        g[-1, :] = 255
+    else:
+        g[:, 0, :] = 255
+        g[:, -1, :] = 255
+        g[0, :, :] = 255
+        g[-1, :, :] = 255
+    name = 'entry-' + ('d3-' if ndim == 3 else '') + f'h{h}-ratio{ratio}-{collision}'
+    return dict(name=name, geometry=g,
+                labels={50: ('PB', 1 + 3 * dp, 1, 0), 200: ('PB', 1.0, 3 if ndim == 2 else 2, 1),
+                        0: ('VD', 0, 0, 0), 100: ('VD', 0, 0, 1), 255: ('SD', 60.0, 0, 0)},
+                model='color', collision=collision, tau=tau, rho=(1.0, 1.0),
+                alpha0=4 / 9 if ndim == 2 else 1 / 3, sigma=sigma, beta=0.7, steps=steps, write=write,
+                height=h, pressure_ratio=ratio, sharp_entry_pressure=pc, pressure_drop=dp)
+
+
+def color_zou_he_cases():
+    """Two-phase Zou-He boundaries, ColorFluid::zouHeBoundary
+    (colorfluid.cpp:638-734): the entry slit in 2D and 3D, a VB inlet with
+    unequal viscosities (per-node MRT rates), and an SRT channel along -y."""
+    out = [entry_case(1.5, 2, steps=400, write=400),
+           entry_case(0.5, 2, collision='SRT', tau=(1.0, 0.8), steps=400, write=400),
+           entry_case(1.5, 3, h=6, nx=25, steps=200, write=200)]
+    c = entry_case(1.5, 2, h=8, nx=33, steps=300, write=300, tau=(1.0, 0.7))
+    c['labels'] = dict(c['labels'])
+    c['labels'][50] = ('VB', 2e-3, 1, 0)
+    c['name'] = 'vb-color-d2-h8-MRT'
+    out.append(c)
+    # Along -y in 3D: VB (phase 1) on the y = ny-1 plane pushing into phase 0,
+    # PB (phase 0) on y = 0; SD walls on the x planes.
+    nx, ny, nz = 8, 20, 4
+    g = np.full((nz, ny, nx), 0, np.uint8)
+    g[:, ny // 2:, :] = 100
+    g[:, 0, :] = 50
+    g[:, -1, :] = 200
+    g[:, :, 0] = 255
+    g[:, :, -1] = 255
+    out.append(dict(name='vb-color-y-d3-SRT', geometry=g,
+                    labels={50: ('PB', 1.0, 3, 0), 200: ('VB', 1e-3, 4, 1), 0: ('VD', 0, 0, 0),
+                            100: ('VD', 0, 0, 1), 255: ('SD', 90.0, 0, 0)},
+                    model='color', collision='SRT', tau=(1.0, 1.0), rho=(1.0, 1.0), alpha0=1 / 3,
+                    sigma=0.003, beta=0.7, steps=200, write=200))
+    return out
+
+
 def pressure_report_channel():
     """scripts/porous_media.py:257-279 (pressure_study): a 16-wide slit between
     SD walls, PB inlet 1 + 3e-5 and outlet 1 along x, MRT tau 1, 6000 steps,
@@ -187,7 +250,7 @@ def golden_cases():
     return ([channel_config1(), channel_mrt(), drop_3d(), wall_color_3d(0.7, 'MRT'),
              wall_color_3d(1.0, 'SRT'), wall_color_2d('MRT'), wall_color_2d('SRT'),
              porous_scsp('MRT'), porous_scsp('SRT'), porous_scsp_2d('MRT')] + force_cases()
-            + zou_he_cases())
+            + zou_he_cases() + color_zou_he_cases())
 
 
 def prm_text(case, grid_file='geometry.raw', out='field', report_dir=0):
