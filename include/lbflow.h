@@ -83,8 +83,9 @@ typedef struct {
     int32_t phase;    /* VD/GV/PB/VB: fluid phase */
     int32_t reserved;
     double value;     /* GV: force magnitude; PB: density; VB: speed along dir
-                         (SCSP::zouHeBoundary, scsp.cpp:188-275; single phase
-                         only); SD: contact angle in degrees */
+                         (SCSP::zouHeBoundary, scsp.cpp:188-275;
+                         ColorFluid::zouHeBoundary, colorfluid.cpp:638-734);
+                         SD: contact angle in degrees */
 } lbf_label;
 
 typedef struct {

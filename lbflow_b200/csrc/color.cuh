@@ -74,34 +74,18 @@ color_phase(const Grid g, const typename S::T* __restrict__ fin, double* __restr
     phi[i] = (double)((d0 - d1) / dt);
 }
 
-// Pass 2: collision, gradient, perturbation and recoloring.
-// COLL: 0 = SRT, 1 = MRT.  PULL = false is the t = 0 collision.
-template <class L, class S, int COLL, bool PULL>
-__global__ void __launch_bounds__(128)
-color_collide(const Grid g, const Force F, const ColorParams P, const ColorWall W,
-              const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
-              const double* __restrict__ phi, Macros mo, const int out, uint32_t* __restrict__ err)
+// Pass 2 for one node whose incoming populations f0, f1 (and the neighbour
+// indices nbr) are gathered: macros, collision, gradient, perturbation and
+// recoloring.  COLL: 0 = SRT, 1 = MRT.
+template <class L, class S, int COLL>
+__device__ __forceinline__ void color_update(const Grid& g, const Force& F, const ColorParams& P,
+                                             const ColorWall& W, typename S::T* __restrict__ fout,
+                                             const double* __restrict__ phi, const Macros& mo, const int out,
+                                             uint32_t* __restrict__ err, const uint32_t i,
+                                             typename S::R (&f0)[L::Q], typename S::R (&f1)[L::Q],
+                                             const uint32_t (&nbr)[L::Q])
 {
     using R = typename S::R;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.nf) return;
-    int x, y, z;
-    unpack(__ldg(&g.coord[i]), x, y, z);
-    R f0[L::Q], f1[L::Q];
-    uint32_t nbr[L::Q];
-    gather<L, S, PULL>(g, fin, i, x, y, z, f0, nbr, R(0));
-    gather<L, S, PULL>(g, fin + (size_t)L::Q * g.nfp, i, x, y, z, f1, nbr, R(0));
-    if (!PULL) {
-        // t = 0: neighbours by direct lookup (the pull above read local values).
-#pragma unroll
-        for (int q = 1; q < L::Q; ++q) {
-            bool fluid;
-            const uint32_t j = lookup(g, wrap(x + L::ex(q), g.nx), wrap(y + L::ey(q), g.ny),
-                                      L::D == 3 ? wrap(z + L::ez(q), g.nz) : 0, fluid);
-            nbr[q] = fluid ? j : 0xffffffffu;
-        }
-    }
-
     // ColorFluid::calcMacroVar (colorfluid.cpp:238-290) and bodyForce (:736-750).
     R d0 = f0[0], d1 = f1[0];
 #pragma unroll
@@ -292,6 +276,209 @@ color_collide(const Grid g, const Force F, const ColorParams P, const ColorWall 
             S::store(o1 + (size_t)q * g.nfp + i, fT[q] - a0, q, R(0));
         }
     }
+}
+
+// Pass 2: collision, gradient, perturbation and recoloring of every fluid node.
+// PULL = false is the t = 0 collision.
+template <class L, class S, int COLL, bool PULL>
+__global__ void __launch_bounds__(128)
+color_collide(const Grid g, const Force F, const ColorParams P, const ColorWall W,
+              const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
+              const double* __restrict__ phi, Macros mo, const int out, uint32_t* __restrict__ err)
+{
+    using R = typename S::R;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.nf) return;
+    int x, y, z;
+    unpack(__ldg(&g.coord[i]), x, y, z);
+    R f0[L::Q], f1[L::Q];
+    uint32_t nbr[L::Q];
+    gather<L, S, PULL>(g, fin, i, x, y, z, f0, nbr, R(0));
+    gather<L, S, PULL>(g, fin + (size_t)L::Q * g.nfp, i, x, y, z, f1, nbr, R(0));
+    if (!PULL) {
+        // t = 0: neighbours by direct lookup (the pull above read local values).
+#pragma unroll
+        for (int q = 1; q < L::Q; ++q) {
+            bool fluid;
+            const uint32_t j = lookup(g, wrap(x + L::ex(q), g.nx), wrap(y + L::ey(q), g.ny),
+                                      L::D == 3 ? wrap(z + L::ez(q), g.nz) : 0, fluid);
+            nbr[q] = fluid ? j : 0xffffffffu;
+        }
+    }
+    color_update<L, S, COLL>(g, F, P, W, fout, phi, mo, out, err, i, f0, f1, nbr);
+}
+
+// ---- two-phase Zou-He boundaries ------------------------------------------------
+// ColorFluid::zouHeBoundary (colorfluid.cpp:638-734) runs after streaming and
+// bounce-back: the single-phase rule applied to the total distribution
+// f0 + f1, with the rebuilt unknowns given to the label's phase and the other
+// phase's unknowns cleared.  Its density and velocity are intermediates --
+// calcMacroVar (whose node set includes PB/VB) recomputes both from the
+// populations -- except in the adjacent-step history of a report, which the
+// reference copies between the two: the velocity there is the boundary's
+// prescribed one and the phase indicator is the previous step's rho0 - rho1
+// over this step's boundary density (colorfluid.cpp:162-167).
+// The step runs as: pass 1 -> boundary phase pass (phi of the boundary nodes
+// from their rebuilt populations) -> pass 2 -> boundary collision pass (the
+// boundary nodes again, overwriting what pass 2 wrote for them).
+// Non-contracted operations in the reference's order.
+template <class L, class R, int DIR>
+__device__ __forceinline__ void color_zou_he_node(R (&f0)[L::Q], R (&f1)[L::Q], uint32_t kind, int phs,
+                                                  double val, R& dens, R& ua)
+{
+    constexpr int A = ZouHeDir<L, DIR>::A, SG = ZouHeDir<L, DIR>::SG;
+    R sum = R(0);
+#pragma unroll
+    for (int q = 1; q < L::Q; ++q)
+        if (comp<L>(q, A) == -SG) sum = xadd(sum, xadd(xadd(xadd(f0[q], f0[q]), f1[q]), f1[q]));
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q)
+        if (comp<L>(q, A) == 0) sum = xadd(sum, xadd(f0[q], f1[q]));
+    if (kind == kZouHeVB) {
+        const double vel = SG > 0 ? val : -val;
+        ua = R(vel);
+        dens = xmul(sum, R(1.0 / (1.0 - vel)));
+    } else {
+        dens = R(val);
+        const R s = xsub(sum / R(val), R(1));
+        ua = SG > 0 ? -s : s;
+    }
+    R fq[L::Q];
+#pragma unroll
+    for (int q = 1; q < L::Q; ++q) {
+        if (comp<L>(q, A) != SG) continue;
+        R fT = xadd(f0[L::op(q)], f1[L::op(q)]);
+        fT = xadd(fT, xmul(xmul(xmul(R(SG), R(6.0 * w<L>(q))), dens), ua));
+        R t = R(0);
+#pragma unroll
+        for (int n = 1; n < L::Q; ++n) {
+            if (comp<L>(n, A) != 0) continue;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                if (d == A || comp<L>(n, d) == 0 || comp<L>(q, d) == 0) continue;
+                if (comp<L>(n, d) == comp<L>(q, d)) t = xadd(t, xadd(f0[n], f1[n]));
+                else t = xsub(t, xadd(f0[n], f1[n]));
+            }
+        }
+        fq[q] = xsub(fT, xmul(t, R(0.5)));
+    }
+#pragma unroll
+    for (int q = 1; q < L::Q; ++q) {
+        if (comp<L>(q, A) != SG) continue;
+        f0[q] = phs == 0 ? fq[q] : R(0);
+        f1[q] = phs == 0 ? R(0) : fq[q];
+    }
+}
+
+// Gather a boundary node and apply the rule; returns the boundary density and
+// axial velocity (ua on axis *axis).
+template <class L, class S>
+__device__ __forceinline__ void color_zou_he_gather(const Grid& g, const ZouHe& z, const uint32_t k,
+                                                    const typename S::T* __restrict__ fin, uint32_t& i,
+                                                    typename S::R (&f0)[L::Q], typename S::R (&f1)[L::Q],
+                                                    uint32_t (&nbr)[L::Q], typename S::R& dens,
+                                                    typename S::R& ua, int& axis)
+{
+    i = __ldg(&z.node[k]);
+    const uint32_t code = __ldg(&z.code[k]);
+    const double val = __ldg(&z.value[k]);
+    int x, y, zc;
+    unpack(__ldg(&g.coord[i]), x, y, zc);
+    gather<L, S, true>(g, fin, i, x, y, zc, f0, nbr, typename S::R(0));
+    gather<L, S, true>(g, fin + (size_t)L::Q * g.nfp, i, x, y, zc, f1, nbr, typename S::R(0));
+    const uint32_t kind = (code >> 8) & 0xffu;
+    const int phs = (int)(code >> 16);
+    const int dir = (int)(code & 0xffu);
+    axis = L::ex(dir) != 0 ? 0 : (L::ey(dir) != 0 ? 1 : 2);
+    switch (dir) {
+    case 1: color_zou_he_node<L, typename S::R, 1>(f0, f1, kind, phs, val, dens, ua); break;
+    case 2: color_zou_he_node<L, typename S::R, 2>(f0, f1, kind, phs, val, dens, ua); break;
+    case 3: color_zou_he_node<L, typename S::R, 3>(f0, f1, kind, phs, val, dens, ua); break;
+    case 4: color_zou_he_node<L, typename S::R, 4>(f0, f1, kind, phs, val, dens, ua); break;
+    default:
+        if constexpr (L::D == 3) {
+            if (dir == 5) color_zou_he_node<L, typename S::R, 5>(f0, f1, kind, phs, val, dens, ua);
+            else color_zou_he_node<L, typename S::R, 6>(f0, f1, kind, phs, val, dens, ua);
+        }
+        break;
+    }
+}
+
+// Boundary phase pass: phi of the boundary nodes from their rebuilt populations.
+template <class L, class S>
+__global__ void __launch_bounds__(128)
+color_zou_he_phase(const Grid g, const ZouHe z, const typename S::T* __restrict__ fin,
+                   double* __restrict__ phi, uint32_t* __restrict__ err)
+{
+    using R = typename S::R;
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= z.n) return;
+    uint32_t i;
+    R f0[L::Q], f1[L::Q], dens, ua;
+    uint32_t nbr[L::Q];
+    int axis;
+    color_zou_he_gather<L, S>(g, z, k, fin, i, f0, f1, nbr, dens, ua, axis);
+    R d0 = f0[0], d1 = f1[0];
+#pragma unroll
+    for (int q = 1; q < L::Q; ++q) { d0 += f0[q]; d1 += f1[q]; }
+    const R dt = d0 + d1;
+    if (!isfinite(d0) || !isfinite(d1) || !isfinite(dt) || !(dt > R(0))) atomicOr(err, kErrDensity);
+    const R tol = sizeof(R) == 8 ? R(1e-10) : R(2.7e-5);
+    if (d0 < -tol * dt || d1 < -tol * dt) atomicOr(err, kErrComponent);
+    phi[i] = (double)((d0 - d1) / dt);
+}
+
+// Boundary collision pass (after pass 2); also keeps the report's adjacent
+// history of the boundary nodes as the reference forms it.  z.num[k] holds
+// rho0 - rho1 of the last step that asked for the adjacent history.
+template <class L, class S, int COLL>
+__global__ void __launch_bounds__(128)
+color_zou_he_collide(const Grid g, const Force F, const ColorParams P, const ColorWall W, const ZouHe z,
+                     const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
+                     const double* __restrict__ phi, Macros mo, const int out, uint32_t* __restrict__ err)
+{
+    using R = typename S::R;
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= z.n) return;
+    uint32_t i;
+    R f0[L::Q], f1[L::Q], dens, ua;
+    uint32_t nbr[L::Q];
+    int axis;
+    color_zou_he_gather<L, S>(g, z, k, fin, i, f0, f1, nbr, dens, ua, axis);
+    R d0 = f0[0], d1 = f1[0];
+#pragma unroll
+    for (int q = 1; q < L::Q; ++q) { d0 += f0[q]; d1 += f1[q]; }
+    color_update<L, S, COLL>(g, F, P, W, fout, phi, mo, out, err, i, f0, f1, nbr);
+    if (out & kOutMacros) {
+        const double prev = z.num[k];
+        mo.indadj[i] = (double)dens > 0.0 ? prev / (double)dens : 0.0;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) mo.uadj[(size_t)a * g.nfp + i] = a == axis ? (double)ua : 0.0;
+    }
+    if (out & kOutAdjacent) z.num[k] = (double)(d0 - d1);
+}
+
+// The adjacent-history numerator at t = 0 (no boundary rule at t = 0; the
+// reference's initial calcMacroVar covers PB/VB).
+template <class L, class S>
+__global__ void __launch_bounds__(128)
+color_zou_he_record(const Grid g, const ZouHe z, const typename S::T* __restrict__ fin)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= z.n) return;
+    const uint32_t i = __ldg(&z.node[k]);
+    double d0 = 0.0, d1 = 0.0;
+    {
+        typename S::R a = S::load(fin + i, 0, typename S::R(0)), b = S::load(fin + (size_t)L::Q * g.nfp + i, 0, typename S::R(0));
+#pragma unroll
+        for (int q = 1; q < L::Q; ++q) {
+            a += S::load(fin + (size_t)q * g.nfp + i, q, typename S::R(0));
+            b += S::load(fin + ((size_t)L::Q + q) * g.nfp + i, q, typename S::R(0));
+        }
+        d0 = (double)a;
+        d1 = (double)b;
+    }
+    z.num[k] = d0 - d1;
 }
 
 // t = 0 populations of ColorFluid::initialize (colorfluid.cpp:214-236):

@@ -13,14 +13,22 @@ void dispatch(bool pull, int out, const ColorLaunch& a)
     T* fout = static_cast<T*>(a.fout);
     const unsigned threads = 128, blocks = blocks_for(a.g.nf, threads);
     if (blocks == 0) return;
+    const unsigned zb = blocks_for(a.zh.n, threads);
     if (pull) color_phase<L, S, true><<<blocks, threads, 0, a.stream>>>(a.g, fin, a.phi, a.err);
     else color_phase<L, S, false><<<blocks, threads, 0, a.stream>>>(a.g, fin, a.phi, a.err);
+    // Zou-He boundary nodes (PB/VB): their phase from the rebuilt populations
+    // before pass 2 reads it, and their collision after pass 2 (overwriting).
+    if (pull && zb) color_zou_he_phase<L, S><<<zb, threads, 0, a.stream>>>(a.g, a.zh, fin, a.phi, a.err);
+    if (!pull && zb && (out & kOutAdjacent)) color_zou_he_record<L, S><<<zb, threads, 0, a.stream>>>(a.g, a.zh, fin);
     if (pull)
         color_collide<L, S, COLL, true><<<blocks, threads, 0, a.stream>>>(
             a.g, a.F, a.P, a.W, fin, fout, a.phi, a.mo, out, a.err);
     else
         color_collide<L, S, COLL, false><<<blocks, threads, 0, a.stream>>>(
             a.g, a.F, a.P, a.W, fin, fout, a.phi, a.mo, out, a.err);
+    if (pull && zb)
+        color_zou_he_collide<L, S, COLL><<<zb, threads, 0, a.stream>>>(a.g, a.F, a.P, a.W, a.zh, fin, fout,
+                                                                      a.phi, a.mo, out, a.err);
 
 }
 

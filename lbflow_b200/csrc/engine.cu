@@ -44,7 +44,7 @@ struct lbf_engine {
     Force force{};
     ZouHe zh{};                     // PB/VB boundary nodes (single phase)
     uint32_t *zh_node = nullptr, *zh_code = nullptr;
-    double* zh_value = nullptr;
+    double *zh_value = nullptr, *zh_num = nullptr;
     ScspParams sp{};
     ColorParams cp{};
     bool initialized = false;
@@ -92,7 +92,8 @@ const int kE19[19][3] = {{0,0,0},{0,0,1},{0,0,-1},{0,1,0},{0,-1,0},{1,0,0},{-1,0
 
 // Voxels that carry populations: the fluid sets of SCSP::initialize /
 // collision and Simulator::buildIb (scsp.cpp:116-134, 374-464;
-// simulator.cpp:399-415).  PB/VB are accepted for the single-phase model only.
+// simulator.cpp:399-415; ColorFluid's initialize / calcMacroVar / collision
+// sets, colorfluid.cpp:220, 244, 323).
 bool is_fluid(int t) { return t == LBF_VD || t == LBF_GV || t == LBF_PB || t == LBF_VB; }
 bool is_solid(int t) { return t == LBF_BB || t == LBF_SD; }
 
@@ -181,7 +182,7 @@ void launch_step(lbf_engine* e, bool pull, int out)
         if (pull && e->zh.n) launch_scsp_zou_he(e->D, (int)e->cfg.storage, a, e->zh);
     } else {
         ColorWall W{e->angle_id, e->angles, e->tib};
-        ColorLaunch a{grid_of(e), e->force, e->cp, W, fin, fout, e->phi, macros_of(e), e->err, e->stream};
+        ColorLaunch a{grid_of(e), e->force, e->cp, W, fin, fout, e->phi, macros_of(e), e->err, e->stream, e->zh};
         launch_color(e->D, (int)e->cfg.storage, (int)e->cfg.collision, pull, out, a);
     }
     e->cur ^= 1;
@@ -400,9 +401,6 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
         if (L.type == 0) return bail(LBF_EINVAL, "geometry label " + std::to_string(l) + " is not defined");
         if (!is_fluid(L.type) && !is_solid(L.type))
             return bail(LBF_EINVAL, "label " + std::to_string(l) + ": only VD, GV, PB, VB, BB and SD labels are supported");
-        if ((L.type == LBF_PB || L.type == LBF_VB) && c.model != LBF_MODEL_SCSP)
-            return bail(LBF_EINVAL, "label " + std::to_string(l) +
-                                        ": PB/VB boundaries are supported for the single-phase model only");
         if ((L.type == LBF_PB || L.type == LBF_VB) && !std::isfinite(L.value))
             return bail(LBF_EINVAL, "Non-finite boundary value.");
         if ((L.type == LBF_PB || L.type == LBF_VB) && (L.dir <= 0 || L.dir >= e->Q))
@@ -463,7 +461,8 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
         const lbf_label& L = labels[nlabel[k]];
         if (L.type != LBF_PB && L.type != LBF_VB) continue;
         zh_node.push_back(k);
-        zh_code.push_back(((L.type == LBF_VB ? kZouHeVB : kZouHePB) << 8) | (uint32_t)L.dir);
+        zh_code.push_back(((uint32_t)L.phase << 16) | ((L.type == LBF_VB ? kZouHeVB : kZouHePB) << 8) |
+                          (uint32_t)L.dir);
         zh_value.push_back(L.value);
     }
 
@@ -527,7 +526,12 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
         LBF_CUDA(cudaMemcpyAsync(e->zh_node, zh_node.data(), zh_node.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, e->stream));
         LBF_CUDA(cudaMemcpyAsync(e->zh_code, zh_code.data(), zh_code.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, e->stream));
         LBF_CUDA(cudaMemcpyAsync(e->zh_value, zh_value.data(), zh_value.size() * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+        if (c.model == LBF_MODEL_COLOR) {
+            LBF_ALLOC(e->zh_num, zh_node.size());
+            LBF_CUDA(cudaMemsetAsync(e->zh_num, 0, zh_node.size() * sizeof(double), e->stream));
+        }
         e->zh.n = (uint32_t)zh_node.size();
+        e->zh.num = e->zh_num;
         e->zh.node = e->zh_node;
         e->zh.code = e->zh_code;
         e->zh.value = e->zh_value;
@@ -666,7 +670,7 @@ void lbf_destroy(lbf_engine* e)
     void* ptrs[] = {e->f[0], e->f[1], e->ex[0], e->ex[1], e->occ, e->coord, e->node_label, e->node_phase, e->label_force,
                     e->rho0, e->rho1, e->u, e->uprev, e->uadj, e->ind, e->indprev, e->indadj,
                     e->phi, e->angle_id, e->angles, e->tib, e->err, e->partial, e->red,
-                    e->zh_node, e->zh_code, e->zh_value};
+                    e->zh_node, e->zh_code, e->zh_value, e->zh_num};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (e->h_red) cudaFreeHost(e->h_red);
     if (e->stream) cudaStreamDestroy(e->stream);

@@ -101,8 +101,6 @@ Simulation::Simulation(const Params& p) : p_(p)
     for (int v = 0; v < 256; ++v) {
         if (!used[v]) continue;
         const LabelType t = p.label(v).type;
-        if ((t == PB || t == VB) && color_)
-            throw std::invalid_argument("Pressure and velocity boundaries (PB/VB) are supported for the single-phase model only.");
         if (t == HF) throw std::invalid_argument("Half-permeable films (HF) are not supported by the B200 engine.");
     }
     // fluid_nodes of the timing line (simulator.cpp:47-56).

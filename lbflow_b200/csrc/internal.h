@@ -33,6 +33,7 @@ struct ColorLaunch {
     Macros mo;
     uint32_t* err;
     cudaStream_t stream;
+    ZouHe zh;          // PB/VB boundary nodes (n = 0: none)
 };
 
 // storage: LBF_STORE_* value; dims: 2 or 3.

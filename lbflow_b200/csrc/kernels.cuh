@@ -412,8 +412,9 @@ scsp_step(const Grid g, const Force F, const ScspParams P,
 struct ZouHe {
     uint32_t n;                          // boundary nodes
     const uint32_t* __restrict__ node;   // compact node index
-    const uint32_t* __restrict__ code;   // kind << 8 | dir (dir 1..2D, the lattice direction)
+    const uint32_t* __restrict__ code;   // phase << 16 | kind << 8 | dir (dir 1..2D, the lattice direction)
     const double* __restrict__ value;    // PB density or VB speed
+    double* num;                         // two-phase only: per-node adjacent-history numerator
 };
 enum : uint32_t { kZouHeVB = 1, kZouHePB = 2 };
 
@@ -511,7 +512,7 @@ scsp_zou_he(const Grid g, const ScspParams P, const ZouHe z,
     uint32_t nbr[L::Q];
     gather<L, S, true>(g, fin, i, x, y, zc, f, nbr, rho0, ein);
 
-    const uint32_t kind = code >> 8;
+    const uint32_t kind = (code >> 8) & 0xffu;
     R u[3];
     R rho = R(0);
     double dens = 0.0;

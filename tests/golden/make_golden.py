@@ -90,7 +90,7 @@ def cli_contracts(exe):
     """Reference behaviour of the command line: error messages of invalid
     inputs, VTI headers, checkpoint sidecars and report lines."""
     from cases import (force_cases, channel_mrt, wall_color_2d, porous_scsp, wall_color_3d, zou_he_cases,
-                       pressure_report_channel)
+                       pressure_report_channel, entry_case)
     import re
     out = {'errors': {}, 'vti_header': {}, 'meta': {}, 'reports': {}}
     base = force_cases()[7]          # force-scsp-d3-MRT-tau1.4
@@ -133,7 +133,8 @@ def cli_contracts(exe):
     for case, rdir in ((dict(porous_scsp('MRT'), report=50, steps=300), 1),
                        (dict(wall_color_3d(0.7, 'MRT'), report=50, steps=200), 1),
                        (dict(zou_he_cases()[0], report=50, steps=300), 1),
-                       (dict(pressure_report_channel(), report=2000), 1)):
+                       (dict(pressure_report_channel(), report=2000), 1),
+                       (dict(entry_case(1.5, 2, steps=400, write=400), report=100), 1)):
         code, stdout, _ = run_ref(exe, case, prm_text(case, report_dir=rdir))
         lines = [l for l in stdout.splitlines() if l.startswith(' - ') or l.startswith('Step ')]
         out['reports'][case['name']] = dict(report_dir=rdir, report=case['report'], steps=case['steps'],

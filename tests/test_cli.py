@@ -16,7 +16,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from cases import (channel_mrt, drop_3d, force_cases, golden_cases, porous_scsp, pressure_report_channel, prm_text,
+from cases import (channel_mrt, drop_3d, golden_cases, porous_scsp, pressure_report_channel, prm_text,
                    wall_color_2d, wall_color_3d)
 from conftest import GOLDEN, fluid_mask, load_golden
 
@@ -82,11 +82,10 @@ def test_unsupported_options_are_refused(tmp_path):
         text = prm_text(case).replace('wallGradient "legacy";', f'{key} {val};')
         code, out = run_cli(tmp_path / key, case, text)
         assert code != 0 and 'not supported by the B200 engine' in out
-    color = force_cases()[-1]
-    text = prm_text(color).replace('75 "GV" "9.9999999999999995e-07" "1" "1"', '75 "PB" "1.0" "1" "1"')
-    assert '"PB"' in text
-    code, out = run_cli(tmp_path / 'pb', color, text)
-    assert code != 0 and 'PB/VB' in out and 'single-phase' in out
+    text = prm_text(case).replace('75 "GV" "9.9999999999999995e-07" "1" "0"', '75 "HF" "N/A" "N/A" "0"')
+    assert '"HF"' in text
+    code, out = run_cli(tmp_path / 'hf', case, text)
+    assert code != 0 and 'HF' in out
 
 
 # ---- GPU runs -----------------------------------------------------------------
