@@ -220,10 +220,12 @@ def main():
                     help='mlups: the throughput line; ttp: time to permeability, plain FP64 vs reduced storage')
     ap.add_argument('--storages', default='fp64,fp32,fp32+acc,bfp16+acc,fp32+warm0')
     ap.add_argument('--max-steps', type=int, default=400000)
-    ap.add_argument('--workload', default='scsp', choices=('scsp', 'color', 'batch', 'operator'),
+    ap.add_argument('--io-write', type=int, default=500, help='io: VTI write interval')
+    ap.add_argument('--io-restart', type=int, default=1000, help='io: checkpoint interval')
+    ap.add_argument('--workload', default='scsp', choices=('scsp', 'color', 'batch', 'operator', 'io'),
                     help='scsp: 256^3 single-phase cube; color: 128x128x256 two-phase color-gradient MRT; '
                          'batch: many uneven geometries in one launch; operator: the warm-start network '
-                         '(forward + backward) on the tensor cores')
+                         '(forward + backward) on the tensor cores; io: output cost of a command-line run')
     ap.add_argument('--count', type=int, default=512, help='batch: number of geometries')
     ap.add_argument('--ttp-media', default='cube', choices=('cube', 'eval192'),
                     help='ttp: the 256^3 cube, or held-out 192^3 media')
@@ -256,6 +258,8 @@ def main():
         return batch_run(args)
     if args.workload == 'operator':
         return operator_run(args)
+    if args.workload == 'io':
+        return io_run(args)
 
     import torch
     import torch.distributed as dist
@@ -392,6 +396,58 @@ def color_throughput(args):
                                         unit='GB/s', bytes_per_node=alg, peak_kind=kind),
                           saturation_phase0=sums[8] / nf, clocks=clocks.summary())))
     eng.close()
+    return 0
+
+
+def io_run(args):
+    """Output cost of a command-line run: the LBFlow binary on the 256^3 cube
+    (FP64 MRT), once writing VTI fields every `--io-write` steps and a
+    checkpoint every `--io-restart` steps, once writing only at the end; the
+    timing line's field and checkpoint seconds per output and the wall-time
+    overhead of the outputs."""
+    import tempfile
+    exe = ROOT / 'lbflow_b200' / 'lib' / 'LBFlow'
+    geometry = make_geometry(args.size, 3.0, 0.22, seed=0)
+    nz, ny, nx = geometry.shape
+    steps, W, R = args.steps, args.io_write, args.io_restart
+
+    def run(write, restart):
+        with tempfile.TemporaryDirectory() as d:
+            d = Path(d)
+            geometry.tofile(d / 'geometry.raw')
+            prm = (f'gridFile "geometry.raw";\ndimension {nz} {ny} {nx};\ndirections 19;\nfileType "uint8";\n'
+                   f'latticeLen 1;\nstartTime 0;\nendTime {steps};\nwriteInterval {write};\n'
+                   f'reportInterval {write};\nrestartInterval {restart};\nstopError 1e-12;\noutPath "field";\n'
+                   f'logPath ".";\nreportDir 0;\nreportSlice 1 {nx - 2};\nfluidModel "scsp";\n'
+                   f'equilModel "MRT";\nrexlationTime 1;\nlatticeSpeed 1;\nalpha0 0.33333333333333331;\n'
+                   f'density 1;\ncontactAngle 90;\nsurfaceTension 0;\ninterfaceThickness 0.7;\n'
+                   f'75 "GV" "1e-5" "1" "0"\n255 "SD" "90" "N/A" "N/A"\n')
+            (d / 'input.prm').write_text(prm)
+            t0 = time.perf_counter()
+            r = subprocess.run([str(exe), 'input.prm'], cwd=d, capture_output=True, text=True)
+            wall = time.perf_counter() - t0
+            if r.returncode != 0:
+                raise RuntimeError('LBFlow failed: ' + r.stdout[-500:])
+            t = [json.loads(l[len('LBFlowTiming '):]) for l in r.stdout.splitlines()
+                 if l.startswith('LBFlowTiming ')][0]
+            files = sorted(p.name for p in d.iterdir() if p.name.startswith('field'))
+            size = sum((d / f).stat().st_size for f in files)
+            return t, wall, files, size
+
+    quiet, wq, _, _ = run(steps, steps * 10)
+    loud, wl, files, size = run(W, R)
+    n_vti = steps // W + 1
+    n_rst = steps // R
+    print(json.dumps(dict(
+        metric='command-line output cost, 256^3 FP64 MRT', unit='s',
+        value=(loud['run_seconds_max'] - quiet['run_seconds_max']) / (n_vti - 2 + n_rst),
+        higher_is_better=False, steps=steps, write_interval=W, restart_interval=R,
+        vti_files=n_vti, checkpoints=n_rst, bytes_written=size,
+        seconds_per_vti=loud['fields_diagnostics_seconds_max'] / n_vti,
+        seconds_per_checkpoint=loud['checkpoint_seconds_max'] / max(n_rst, 1),
+        run_seconds_with_outputs=loud['run_seconds_max'], run_seconds_final_only=quiet['run_seconds_max'],
+        numerical_seconds=[loud['numerical_seconds_max'], quiet['numerical_seconds_max']],
+        process_wall_seconds=[wl, wq])))
     return 0
 
 

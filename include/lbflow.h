@@ -63,7 +63,9 @@ enum {
     LBF_ERR_DENSITY = 1u << 0,    /* non-finite or non-positive density */
     LBF_ERR_COMPONENT = 1u << 1,  /* negative component density (color) */
     LBF_ERR_TAU = 1u << 2,        /* local relaxation time <= 0.5 (color) */
-    LBF_ERR_VELOCITY = 1u << 3    /* non-finite velocity (color) */
+    LBF_ERR_VELOCITY = 1u << 3,   /* non-finite velocity (color) */
+    LBF_ERR_OUTPUT = 1u << 4      /* non-finite population met by
+                                     lbf_populations_dense_async */
 };
 
 /* lbf_step flags: what the LAST step of the call also writes. */
@@ -177,6 +179,33 @@ int lbf_set_populations(lbf_engine *e, const double *host, size_t n);
  * only; may be NULL), u [3][voxel]; zero on solid voxels as in the VTI output
  * (filevti.cpp:113-172).  Any pointer may be NULL. */
 int lbf_get_macros(lbf_engine *e, double *rho0, double *rho1, double *u);
+
+/* Output without a host round trip per voxel: the dense arrays of
+ * lbf_get_macros / lbf_get_populations written by the device, enqueued on the
+ * engine's stream (the call returns at once; lbf_synchronize or lbf_status
+ * waits).  `out` must be memory the device can write: device memory of the
+ * engine's device, or page-locked host memory (lbf_host_alloc, or any
+ * cudaHostAlloc/cudaHostRegister memory); pageable memory is refused.  Keep
+ * it alive and unread until the wait returns.
+ *
+ * lbf_fields_dense_async replaces the field gathering of FileVti::Save
+ * (filevti.cpp:113-172): out holds, for N = nx*ny*nz voxels, rho0 [N], then
+ * rho1 [N] for the color model, then the velocity [N][dims] with components
+ * x, y(, z) interleaved -- the appended arrays of the VTI file in order.
+ * n = (1 + color + dims) * N.  Zero on solid voxels.
+ *
+ * lbf_populations_dense_async replaces the gathering of saveRst
+ * (scsp.cpp:277-302; colorfluid.cpp:766-812): out = [phase][q][voxel] FP64,
+ * n = phases*Q*N, solid voxels 0, the bytes of the .rst file.  A non-finite
+ * value sets LBF_ERR_OUTPUT in the error word (the reference refuses to
+ * write such a checkpoint, simulator.cpp:327-333). */
+int lbf_fields_dense_async(lbf_engine *e, double *out, size_t n);
+int lbf_populations_dense_async(lbf_engine *e, double *out, size_t n);
+
+/* Page-locked host memory the device can write (cudaHostAlloc, portable and
+ * mapped), for the two calls above. */
+int lbf_host_alloc(size_t bytes, void **out);
+void lbf_host_free(void *p);
 
 /* Device reductions of Simulator::updateConvergence (simulator.cpp:248-325).
  * first != 0 only records the current velocity (and phase indicator) as the

@@ -13,7 +13,7 @@ from pathlib import Path
 
 import numpy as np
 
-__all__ = ['Engine', 'LbfError', 'library', 'library_path', 'LABEL_TYPES', 'ensure_built']
+__all__ = ['Engine', 'HostBuffer', 'LbfError', 'library', 'library_path', 'LABEL_TYPES', 'ensure_built']
 
 PKG = Path(__file__).resolve().parent
 _LIB_PATH = PKG / 'lib' / 'liblbflow_b200.so'
@@ -29,7 +29,8 @@ STEP_ADJACENT = 2
 ERR_BITS = {1: 'Non-finite or non-positive fluid density.',
             2: 'Negative component density outside roundoff tolerance.',
             4: 'Invalid local relaxation time.',
-            8: 'Non-finite fluid velocity.'}
+            8: 'Non-finite fluid velocity.',
+            16: 'Non-finite post-collision population; no restart will be written.'}
 
 
 class LbfError(RuntimeError):
@@ -97,6 +98,10 @@ def library():
             'lbf_synchronize': (I, [P]),
             'lbf_stream': (P, [P]),
             'lbf_flux_sums_noalloc': (I, [P, P, P, U32, U32, P, P]),
+            'lbf_fields_dense_async': (I, [P, P, ctypes.c_size_t]),
+            'lbf_populations_dense_async': (I, [P, P, ctypes.c_size_t]),
+            'lbf_host_alloc': (I, [ctypes.c_size_t, ctypes.POINTER(P)]),
+            'lbf_host_free': (None, [P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -116,6 +121,33 @@ def make_labels(labels):
     for k, (t, value, d, ph) in labels.items():
         arr[int(k)] = _Label(LABEL_TYPES[t] if isinstance(t, str) else int(t), int(d), int(ph), 0, float(value))
     return arr
+
+
+class HostBuffer:
+    """Page-locked host memory the device can write (lbf_host_alloc), viewed
+    as a float64 numpy array; the destination of the engine's *_dense_async
+    outputs."""
+
+    def __init__(self, count):
+        self._lib = library()
+        self.ptr = ctypes.c_void_p()
+        rc = self._lib.lbf_host_alloc(int(count) * 8, ctypes.byref(self.ptr))
+        if rc != 0:
+            raise LbfError(rc, self._lib.lbf_last_error(None).decode())
+        self.count = int(count)
+        self.array = np.ctypeslib.as_array((ctypes.c_double * self.count).from_address(self.ptr.value))
+
+    def close(self):
+        if self.ptr:
+            self.array = None
+            self._lib.lbf_host_free(self.ptr)
+            self.ptr = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 class Engine:
@@ -256,6 +288,16 @@ class Engine:
     def set_populations(self, f):
         f = np.ascontiguousarray(f, dtype=np.float64).ravel()
         self._ck(self._lib.lbf_set_populations(self._h, _dptr(f), f.size))
+
+    def fields_dense_async(self, address, count):
+        """Enqueue the dense VTI-layout fields into device-writable memory at
+        `address` (a HostBuffer's ptr or a CUDA tensor's data_ptr())."""
+        self._ck(self._lib.lbf_fields_dense_async(self._h, ctypes.c_void_p(int(address)), int(count)))
+
+    def populations_dense_async(self, address, count):
+        """Enqueue the dense checkpoint-layout populations into
+        device-writable memory at `address`."""
+        self._ck(self._lib.lbf_populations_dense_async(self._h, ctypes.c_void_p(int(address)), int(count)))
 
     def macros(self):
         """(rho0, rho1 or None, u[3]) dense, shaped like the geometry."""

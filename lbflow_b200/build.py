@@ -73,7 +73,7 @@ def build(force=False, verbose=False, jobs=None):
     exe = LIB / 'LBFlow'
     hsrc = [HOST / u for u in HOST_UNITS]
     if all(p.exists() for p in hsrc) and (force or _newer(exe, hsrc + _headers(HOST) + [lib])):
-        _run(['g++', '-std=c++11', '-O2', '-Wall', '-I', str(ROOT / 'include'), '-o', str(exe)]
+        _run(['g++', '-std=c++11', '-O2', '-Wall', '-pthread', '-I', str(ROOT / 'include'), '-o', str(exe)]
              + [str(p) for p in hsrc]
              + ['-L', str(LIB), '-llbflow_b200', '-Wl,-rpath,$ORIGIN'])
     return lib

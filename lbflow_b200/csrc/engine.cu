@@ -38,6 +38,7 @@ struct lbf_engine {
     double* tib = nullptr;
     uint32_t* err = nullptr;
     double* partial = nullptr;
+    double* dense_tmp = nullptr;    // FP64 copy of reduced-precision populations (dense output)
     double* red = nullptr;
     double* h_red = nullptr;        // pinned
     cudaStream_t stream = nullptr;
@@ -351,6 +352,70 @@ int expand_to_host(lbf_engine* e, std::vector<double>& compact)
 namespace lbf {
 void set_global_error(const std::string& msg) { g_create_error = msg; }
 }  // namespace lbf
+
+namespace {
+// Dense outputs, one thread per voxel (grid-stride), x fastest, so that a
+// warp writes consecutive addresses of every array.
+__global__ void fields_dense_kernel(const lbf::Grid g, const double* __restrict__ rho0,
+                                    const double* __restrict__ rho1, const double* __restrict__ u, int D,
+                                    double* __restrict__ out, size_t N)
+{
+    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < N; v += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(v % g.nx);
+        const int y = (int)((v / g.nx) % g.ny);
+        const int z = (int)(v / ((size_t)g.nx * g.ny));
+        bool fluid;
+        const uint32_t k = lbf::lookup(g, x, y, z, fluid);
+        out[v] = fluid ? rho0[k] : 0.0;
+        size_t o = N;
+        if (rho1) {
+            out[N + v] = fluid ? rho1[k] : 0.0;
+            o += N;
+        }
+        for (int c = 0; c < D; ++c) out[o + v * D + c] = fluid ? u[(size_t)c * g.nfp + k] : 0.0;
+    }
+}
+
+__global__ void populations_dense_kernel(const lbf::Grid g, const double* __restrict__ in, int blocks,
+                                         double* __restrict__ out, size_t N, uint32_t* __restrict__ err)
+{
+    bool bad = false;
+    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < N; v += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(v % g.nx);
+        const int y = (int)((v / g.nx) % g.ny);
+        const int z = (int)(v / ((size_t)g.nx * g.ny));
+        bool fluid;
+        const uint32_t k = lbf::lookup(g, x, y, z, fluid);
+        for (int b = 0; b < blocks; ++b) {
+            const double val = fluid ? in[(size_t)b * g.nfp + k] : 0.0;
+            bad |= !isfinite(val);
+            out[(size_t)b * N + v] = val;
+        }
+    }
+    if (bad) atomicOr(err, lbf::kErrOutput);
+}
+
+// The device address of a caller buffer, or nullptr when the device cannot
+// write it (pageable host memory, another device's memory).
+double* device_writable(lbf_engine* e, double* p)
+{
+    cudaPointerAttributes pa{};
+    if (cudaPointerGetAttributes(&pa, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (pa.type == cudaMemoryTypeDevice) return pa.device == e->cfg.device ? p : nullptr;
+    if (pa.type == cudaMemoryTypeManaged) return p;
+    if (pa.type == cudaMemoryTypeHost) return static_cast<double*>(pa.devicePointer);
+    return nullptr;
+}
+
+unsigned dense_blocks(size_t N)
+{
+    const size_t b = (N + 255) / 256;
+    return (unsigned)(b < (size_t)148 * 16 ? b : (size_t)148 * 16);
+}
+}  // namespace
 
 extern "C" {
 
@@ -670,7 +735,7 @@ void lbf_destroy(lbf_engine* e)
     void* ptrs[] = {e->f[0], e->f[1], e->ex[0], e->ex[1], e->occ, e->coord, e->node_label, e->node_phase, e->label_force,
                     e->rho0, e->rho1, e->u, e->uprev, e->uadj, e->ind, e->indprev, e->indadj,
                     e->phi, e->angle_id, e->angles, e->tib, e->err, e->partial, e->red,
-                    e->zh_node, e->zh_code, e->zh_value, e->zh_num};
+                    e->zh_node, e->zh_code, e->zh_value, e->zh_num, e->dense_tmp};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (e->h_red) cudaFreeHost(e->h_red);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -873,6 +938,66 @@ int lbf_set_populations(lbf_engine* e, const double* host, size_t n)
     }
     e->initialized = true;
     return LBF_OK;
+}
+
+
+int lbf_fields_dense_async(lbf_engine* e, double* out, size_t n)
+{
+    if (!e || !out) return fail(e, LBF_EINVAL, "NULL argument");
+    const bool color = e->cfg.model == LBF_MODEL_COLOR;
+    if (n != (size_t)(1 + (color ? 1 : 0) + e->D) * e->N)
+        return fail(e, LBF_EINVAL, "fields buffer must hold (1 + color + dims) * nx*ny*nz doubles");
+    int rc = setdev(e);
+    if (rc) return rc;
+    double* d = device_writable(e, out);
+    if (!d) return fail(e, LBF_EINVAL, "out must be device memory of the engine's device or page-locked host memory");
+    if (e->N == 0) return LBF_OK;
+    fields_dense_kernel<<<dense_blocks(e->N), 256, 0, e->stream>>>(grid_of(e), e->rho0, color ? e->rho1 : nullptr,
+                                                                    e->u, e->D, d, e->N);
+    LBF_CK(e, cudaGetLastError());
+    return LBF_OK;
+}
+
+int lbf_populations_dense_async(lbf_engine* e, double* out, size_t n)
+{
+    if (!e || !out) return fail(e, LBF_EINVAL, "NULL argument");
+    const size_t blocks = (size_t)e->phases * e->Q;
+    if (n != blocks * e->N) return fail(e, LBF_EINVAL, "population buffer must hold phases*Q*N doubles");
+    int rc = setdev(e);
+    if (rc) return rc;
+    double* d = device_writable(e, out);
+    if (!d) return fail(e, LBF_EINVAL, "out must be device memory of the engine's device or page-locked host memory");
+    const double* src = static_cast<const double*>(e->f[e->cur]);
+    if (e->cfg.storage != LBF_STORE_FP64) {
+        if (!e->dense_tmp && (rc = dalloc(e, &e->dense_tmp, blocks * e->nfp))) return rc;
+        if (e->D == 3) convert<D3Q19>(e, true, e->f[e->cur], e->dense_tmp);
+        else convert<D2Q9>(e, true, e->f[e->cur], e->dense_tmp);
+        LBF_CK(e, cudaGetLastError());
+        src = e->dense_tmp;
+    }
+    if (e->N == 0) return LBF_OK;
+    populations_dense_kernel<<<dense_blocks(e->N), 256, 0, e->stream>>>(grid_of(e), src, (int)blocks, d, e->N,
+                                                                        e->err);
+    LBF_CK(e, cudaGetLastError());
+    return LBF_OK;
+}
+
+int lbf_host_alloc(size_t bytes, void** out)
+{
+    if (!out) return fail(nullptr, LBF_EINVAL, "lbf_host_alloc: out is NULL");
+    *out = nullptr;
+    const cudaError_t r = cudaHostAlloc(out, bytes ? bytes : 1, cudaHostAllocPortable | cudaHostAllocMapped);
+    if (r != cudaSuccess) {
+        *out = nullptr;
+        return fail(nullptr, r == cudaErrorMemoryAllocation ? LBF_ENOMEM : LBF_ECUDA,
+                    std::string("cudaHostAlloc: ") + cudaGetErrorString(r));
+    }
+    return LBF_OK;
+}
+
+void lbf_host_free(void* p)
+{
+    if (p) cudaFreeHost(p);
 }
 
 int lbf_get_macros(lbf_engine* e, double* rho0, double* rho1, double* u)

@@ -1,6 +1,9 @@
 // File formats (see io.h).
 #include "io.h"
 
+#include <fcntl.h>
+#include <unistd.h>
+
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -29,15 +32,42 @@ std::string stepName(const std::string& outPath, std::size_t t, const char* ext)
 }
 
 namespace {
-void put(std::FILE* f, const void* p, std::size_t bytes)
-{
-    if (bytes && std::fwrite(p, 1, bytes, f) != bytes)
-        throw std::runtime_error("FileRaw::Save() - Failed to save to file");
-}
+// Output file written sequentially with write(2) straight from the caller's
+// buffer (no stdio copy), with every failure reported.
+class Sink {
+public:
+    Sink(const std::string& path, const char* openError) : fd_(::open(path.c_str(), O_WRONLY | O_CREAT | O_TRUNC, 0644))
+    {
+        if (fd_ < 0) throw std::runtime_error(openError);
+    }
+    ~Sink() { if (fd_ >= 0) ::close(fd_); }
+    void put(const void* p, std::size_t bytes, const char* error)
+    {
+        const char* c = static_cast<const char*>(p);
+        while (bytes) {
+            const ssize_t w = ::write(fd_, c, bytes);
+            if (w <= 0) throw std::runtime_error(error);
+            c += w;
+            bytes -= (std::size_t)w;
+        }
+    }
+    void close(const char* error)
+    {
+        const int fd = fd_;
+        fd_ = -1;
+        if (::close(fd) != 0) throw std::runtime_error(error);
+    }
+private:
+    int fd_;
+};
+
+const char kSaveError[] = "FileRaw::Save() - Failed to save to file";
 }  // namespace
 
-void writeVti(const std::string& path, const std::vector<std::size_t>& sz,
-              const std::vector<VtiField>& scalars, const VtiField& vec)
+namespace {
+// VTK ImageData XML header up to the start of the appended data.
+std::string vtiHeader(const std::vector<std::size_t>& sz, const std::vector<std::string>& scalars,
+                      const std::string& vector, int components)
 {
     const std::size_t D = sz.size();
     std::size_t N = 1;
@@ -50,51 +80,51 @@ void writeVti(const std::string& path, const std::vector<std::size_t>& sz,
     h << "<VTKFile type=\"ImageData\" version=\"1.0\" byte_order=\"LittleEndian\" header_type=\"UInt64\">"
       << "<ImageData WholeExtent=\" " << ext.str() << "\" Origin=\"0 0 0\" Spacing=\"1 1 1\">"
       << "<Piece Extent=\"" << ext.str() << "\"><PointData Scalars=\"";
-    for (const VtiField& s : scalars) h << s.name << " ";
-    h << "\" Vectors=\"" << vec.name << " \" >";
+    for (const std::string& s : scalars) h << s << " ";
+    h << "\" Vectors=\"" << vector << " \" >";
     std::size_t offset = 0;
-    for (const VtiField& s : scalars) {
-        h << "<DataArray type=\"Float64\" Name=\"" << s.name << "\" format=\"appended\" offset=\""
+    for (const std::string& s : scalars) {
+        h << "<DataArray type=\"Float64\" Name=\"" << s << "\" format=\"appended\" offset=\""
           << offset << "\"/>";
         offset += N * sizeof(double) + sizeof(uint64_t);
     }
-    h << "<DataArray type=\"Float64\" Name=\"" << vec.name << "\" NumberOfComponents=\"" << vec.components
+    h << "<DataArray type=\"Float64\" Name=\"" << vector << "\" NumberOfComponents=\"" << components
       << "\" format=\"appended\" offset=\"" << offset << "\"/>";
     h << "</PointData><CellData></CellData></Piece></ImageData><AppendedData encoding=\"raw\">_";
-    const std::string head = h.str();
+    return h.str();
+}
+}  // namespace
 
-    std::FILE* f = std::fopen(path.c_str(), "wb");
-    if (!f) throw std::runtime_error("FileRaw::Save() - Can not open file for output.");
-    try {
-        put(f, head.data(), head.size());
-        for (const VtiField& s : scalars) {
-            const uint64_t len = N * sizeof(double);
-            put(f, &len, sizeof len);
-            put(f, s.data, len);
-        }
-        const uint64_t len = N * vec.components * sizeof(double);
-        put(f, &len, sizeof len);
-        std::vector<double> inter((std::size_t)vec.components * N);
-        for (std::size_t i = 0; i < N; ++i)
-            for (int c = 0; c < vec.components; ++c) inter[i * vec.components + c] = vec.data[(std::size_t)c * N + i];
-        put(f, inter.data(), len);
-        const char foot[] = "</AppendedData></VTKFile>";
-        put(f, foot, sizeof foot - 1);
-    } catch (...) {
-        std::fclose(f);
-        throw;
+void writeVtiBlocks(const std::string& path, const std::vector<std::size_t>& sz,
+                    const std::vector<std::string>& scalars, const std::string& vector, int components,
+                    const double* data)
+{
+    std::size_t N = 1;
+    for (std::size_t n : sz) N *= n;
+    const std::string head = vtiHeader(sz, scalars, vector, components);
+    Sink f(path, "FileRaw::Save() - Can not open file for output.");
+    f.put(head.data(), head.size(), kSaveError);
+    std::size_t at = 0;
+    for (std::size_t k = 0; k < scalars.size(); ++k, at += N) {
+        const uint64_t len = N * sizeof(double);
+        f.put(&len, sizeof len, kSaveError);
+        f.put(data + at, len, kSaveError);
     }
-    std::fclose(f);
+    const uint64_t len = N * components * sizeof(double);
+    f.put(&len, sizeof len, kSaveError);
+    f.put(data + at, len, kSaveError);
+    const char foot[] = "</AppendedData></VTKFile>";
+    f.put(foot, sizeof foot - 1, kSaveError);
+    f.close(kSaveError);
 }
 
 void writeCheckpoint(const std::string& path, const double* f, std::size_t count)
 {
     // prepareRestart (simulator.cpp:335-343): truncate, drop the old sidecar.
     std::remove((path + ".meta").c_str());
-    std::FILE* out = std::fopen(path.c_str(), "wb");
-    if (!out) throw std::runtime_error("Cannot create restart population file.");
-    try { put(out, f, count * sizeof(double)); } catch (...) { std::fclose(out); throw; }
-    std::fclose(out);
+    Sink out(path, "Cannot create restart population file.");
+    out.put(f, count * sizeof(double), kSaveError);
+    out.close(kSaveError);
 }
 
 void writeCheckpointMeta(const std::string& path, std::size_t t, std::size_t phases, std::size_t D,

@@ -24,15 +24,12 @@ namespace lbfhost {
 
 std::vector<uint8_t> loadGeometry(const std::string& path, std::size_t n);
 
-struct VtiField {
-    std::string name;
-    int components;                 // 1 (scalar) or D (vector)
-    const double* data;             // scalar: [N]; vector: [3][N] x, y, z planes
-};
-
+// A VTI file from one dense block laid out as its appended arrays: every
+// scalar [N] in order, then the vector [N][components] interleaved.
 // sz: reference order sizes ({y,x} or {z,y,x}).
-void writeVti(const std::string& path, const std::vector<std::size_t>& sz,
-              const std::vector<VtiField>& scalars, const VtiField& vector);
+void writeVtiBlocks(const std::string& path, const std::vector<std::size_t>& sz,
+                    const std::vector<std::string>& scalars, const std::string& vector, int components,
+                    const double* data);
 
 std::string stepName(const std::string& outPath, std::size_t t, const char* ext);
 

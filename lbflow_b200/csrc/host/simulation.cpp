@@ -158,38 +158,85 @@ Simulation::Simulation(const Params& p) : p_(p)
     }
 }
 
+BackgroundWriter::~BackgroundWriter()
+{
+    if (thread_.joinable()) thread_.join();
+    lbf_host_free(buf_);
+}
+
+void BackgroundWriter::wait()
+{
+    if (thread_.joinable()) thread_.join();
+    if (error_) {
+        std::exception_ptr e = error_;
+        error_ = nullptr;
+        std::rethrow_exception(e);
+    }
+}
+
+double* BackgroundWriter::buffer(std::size_t count)
+{
+    if (count > cap_) {
+        lbf_host_free(buf_);
+        buf_ = nullptr;
+        cap_ = 0;
+        void* p = nullptr;
+        if (lbf_host_alloc(count * sizeof(double), &p) != LBF_OK)
+            throw std::runtime_error(std::string("output buffer: ") + lbf_last_error(nullptr));
+        buf_ = static_cast<double*>(p);
+        cap_ = count;
+    }
+    return buf_;
+}
+
 Simulation::~Simulation()
 {
+    // Finish the files in flight (their failures no longer matter here), then
+    // release the engine.
+    try { fieldWriter_.wait(); } catch (...) {}
+    try { checkpointWriter_.wait(); } catch (...) {}
     if (e_) lbf_destroy(e_);
 }
 
+// Output::Save (filevti.cpp:39-172): the device writes the dense arrays into a
+// page-locked buffer; the file is written in the background.
 void Simulation::saveFields(std::size_t t)
 {
-    std::vector<double> r0(N_), r1(color_ ? N_ : 0), u(3 * N_);
-    check(lbf_get_macros(e_, r0.data(), color_ ? r1.data() : nullptr, u.data()), "lbf_get_macros");
-    std::vector<VtiField> scalars;
-    if (color_) {
-        scalars.push_back(VtiField{"r0", 1, r0.data()});
-        scalars.push_back(VtiField{"r1", 1, r1.data()});
-    } else {
-        scalars.push_back(VtiField{"density", 1, r0.data()});
-    }
-    writeVti(stepName(p_.outPath(), t, ".vti"), sz_, scalars,
-             VtiField{color_ ? "v" : "velocity", (int)D_, u.data()});
+    fieldWriter_.wait();
+    const std::size_t n = (1 + (color_ ? 1 : 0) + D_) * N_;
+    double* buf = fieldWriter_.buffer(n);
+    check(lbf_fields_dense_async(e_, buf, n), "lbf_fields_dense_async");
+    check(lbf_synchronize(e_), "lbf_synchronize");
+    const std::vector<std::string> scalars = color_ ? std::vector<std::string>{"r0", "r1"}
+                                                    : std::vector<std::string>{"density"};
+    const std::string path = stepName(p_.outPath(), t, ".vti");
+    const std::vector<std::size_t> sz = sz_;
+    const std::string vec = color_ ? "v" : "velocity";
+    const int comps = (int)D_;
+    fieldWriter_.start([path, sz, scalars, vec, comps, buf]() { writeVtiBlocks(path, sz, scalars, vec, comps, buf); });
 }
 
+// saveRst (scsp.cpp:277-302; colorfluid.cpp:766-812) with the finite check of
+// validatePopulations (simulator.cpp:327-333) done by the device; the sidecar
+// follows the population file in the background write.
 void Simulation::saveCheckpoint(std::size_t t)
 {
     checkDevice();
+    checkpointWriter_.wait();
     const std::size_t count = phases_ * Q_ * N_;
-    std::vector<double> f(count);
-    check(lbf_get_populations(e_, f.data(), count), "lbf_get_populations");
-    for (double v : f)
-        if (!std::isfinite(v))
-            throw std::runtime_error("Non-finite post-collision population; no restart will be written.");
+    double* buf = checkpointWriter_.buffer(count);
+    check(lbf_populations_dense_async(e_, buf, count), "lbf_populations_dense_async");
+    uint32_t bits = 0;
+    check(lbf_status(e_, &bits), "lbf_status");
+    if (bits & LBF_ERR_OUTPUT)
+        throw std::runtime_error("Non-finite post-collision population; no restart will be written.");
     const std::string name = stepName(p_.outPath(), t, ".rst");
-    writeCheckpoint(name, f.data(), count);
-    writeCheckpointMeta(name, t, phases_, D_, Q_, sz_);
+    const std::size_t phases = phases_, D = D_, Q = Q_;
+    const std::vector<std::size_t> sz = sz_;
+    checkpointWriter_.start([name, buf, count, t, phases, D, Q, sz]() {
+        writeCheckpoint(name, buf, count);
+        writeCheckpointMeta(name, t, phases, D, Q, sz);
+    });
 }
 
 void Simulation::loadCheckpoint(std::size_t t)
@@ -362,6 +409,13 @@ void Simulation::run(std::ostream& log)
         completed_ += n;
         if (converged) break;
     }
+    // The files still being written belong to their output categories.
+    double b = StepLog::now();
+    fieldWriter_.wait();
+    seconds_[FIELD_T] += StepLog::now() - b;
+    b = StepLog::now();
+    checkpointWriter_.wait();
+    seconds_[CHECKPOINT_T] += StepLog::now() - b;
     writeTiming(log, StepLog::now() - runStart);
 }
 

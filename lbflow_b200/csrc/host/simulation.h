@@ -4,8 +4,10 @@
 
 #include <chrono>
 #include <cstdint>
+#include <exception>
 #include <ostream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "lbflow.h"
@@ -25,6 +27,29 @@ private:
     std::ostream& os_;
     double t0_;
     bool auto_ = false;
+};
+
+// One file write in the background at a time, from a page-locked buffer the
+// device fills (lbf_fields_dense_async / lbf_populations_dense_async), so the
+// steps that follow an output run while the file is written.
+class BackgroundWriter {
+public:
+    ~BackgroundWriter();
+    // Joins the previous write and rethrows its failure.
+    void wait();
+    // A buffer of at least `count` doubles (kept across writes).
+    double* buffer(std::size_t count);
+    template <class F> void start(F&& write)
+    {
+        thread_ = std::thread([this, write]() {
+            try { write(); } catch (...) { error_ = std::current_exception(); }
+        });
+    }
+private:
+    std::thread thread_;
+    std::exception_ptr error_;
+    double* buf_ = nullptr;
+    std::size_t cap_ = 0;
 };
 
 class Simulation {
@@ -51,6 +76,7 @@ private:
     std::vector<std::size_t> sz_;      // reference order sizes
     std::vector<uint8_t> geometry_;
     lbf_engine* e_ = nullptr;
+    BackgroundWriter fieldWriter_, checkpointWriter_;
     double fluidNodes_ = 0;
     double seconds_[4] = {0, 0, 0, 0}; // INIT, NUMERICAL, FIELD, CHECKPOINT
     std::size_t completed_ = 0;

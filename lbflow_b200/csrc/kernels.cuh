@@ -25,6 +25,7 @@ enum : uint32_t {
     kErrComponent = 1u << 1,  // negative component density (colorfluid.cpp:258-259)
     kErrTau       = 1u << 2,  // local relaxation time <= 0.5 (colorfluid.cpp:269-270)
     kErrVelocity  = 1u << 3,  // non-finite velocity (colorfluid.cpp:282-283)
+    kErrOutput    = 1u << 4,  // non-finite population in a dense checkpoint copy (simulator.cpp:327-333)
 };
 
 // Output requests for a step kernel.
