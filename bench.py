@@ -233,7 +233,8 @@ def main():
     ap.add_argument('--media-index', default=None, help='ttp eval192: comma-separated media indices instead')
     ap.add_argument('--op-conv-only', action='store_true', help='operator: only the single-convolution roofline '
                                                                  '(3 warm-up + 20 timed launches)')
-    ap.add_argument('--report', type=int, default=1000, help='ttp: report interval in steps')
+    ap.add_argument('--report', type=int, default=500, help='ttp: report interval in steps (the +acc '
+                                                            'corrections act on report steps)')
     ap.add_argument('--block', type=int, default=2, help='ttp: block edge of the Darcy corrections (warm start, +acc)')
     ap.add_argument('--accel-at', default='500', help='ttp: report steps (step or step:block, comma separated) at '
                                                       'which +acc runs apply the block Darcy pressure correction')
@@ -527,8 +528,8 @@ def ttp_media(args):
 
 
 def time_to_permeability(args):
-    """Wall time to LBFlow's convergence criterion (report every 1000 steps,
-    relative velocity change < 1e-6 three times in a row) and to K within 1e-3
+    """Wall time to LBFlow's convergence criterion (report every --report
+    steps, relative velocity change < 1e-6 three times in a row) and to K within 1e-3
     of the plain FP64 result, for each run of --storages: a storage name
     (fp64, fp32, fp16, bf16, bfp16) starts from rest as LBFlow does; a
     '+warm' suffix starts from the learned warm start (feature computation,

@@ -49,6 +49,7 @@ struct lbf_engine {
     ScspParams sp{};
     ColorParams cp{};
     bool initialized = false;
+    uint32_t steps = 0;             // pull steps launched (seeds the 16-bit stochastic rounding)
     uint64_t bytes = 0;
     std::string last_error;
 };
@@ -175,6 +176,11 @@ void launch_step(lbf_engine* e, bool pull, int out)
     const void* fin = e->f[e->cur];
     void* fout = e->f[e->cur ^ 1];
     if (e->cfg.model == LBF_MODEL_SCSP) {
+        // FP16 / BF16 storage rounds stochastically, with a fresh seed every
+        // step (deterministic for a given run); the t = 0 collision rounds to
+        // nearest.
+        const bool dither = e->cfg.storage == LBF_STORE_FP16 || e->cfg.storage == LBF_STORE_BF16;
+        e->sp.seed = dither && pull ? (++e->steps * 2654435761u) | 1u : 0u;
         ScspLaunch a{grid_of(e), e->force, e->sp, fin, fout, macros_of(e), e->err, e->stream,
                      e->ex[e->cur], e->ex[e->cur ^ 1], out};
         launch_scsp(e->D, (int)e->cfg.storage, e->cfg.collision == LBF_MRT, pull, out, a);

@@ -75,6 +75,7 @@ __device__ __forceinline__ uint32_t lookup(const Grid& g, int x, int y, int z, b
 // Full FP64 populations (the plain path; arithmetic close to the reference).
 struct StoreF64 {
     static constexpr bool blocked = false;
+    static constexpr bool dither = false;
     using T = double;
     using R = double;
     static constexpr bool shifted = false;
@@ -87,24 +88,49 @@ template <class L> struct ShiftScale {
     __device__ static float scale(int q) { return 4096.0f * 36.0f / (float)L::w36f(q); }
     __device__ static float inv(int q) { return (float)L::w36f(q) / (36.0f * 4096.0f); }
 };
+// Stochastic rounding of a float to a narrower float format that keeps the
+// float's exponent field layout: `drop` low mantissa bits are discarded;
+// adding `drop` random bits before truncating rounds up with probability
+// equal to the discarded fraction, so the stored value is unbiased.  This
+// keeps slow modes whose per-step change is below half a unit in the last
+// place evolving, where round-to-nearest would freeze them.
+__device__ __forceinline__ float dither_bits(float x, uint32_t r, int drop)
+{
+    return __uint_as_float(__float_as_uint(x) + (r >> (32 - drop)));
+}
+
 template <class L> struct StoreF16 {
     static constexpr bool blocked = false;
+    static constexpr bool dither = true;
     using T = __half;
     using R = float;
     static constexpr bool shifted = true;
     __device__ static R load(const T* p, int q, R) { return __half2float(__ldg(p)) * ShiftScale<L>::inv(q); }
     __device__ static void store(T* p, R v, int q, R) { *p = __float2half_rn(v * ShiftScale<L>::scale(q)); }
+    // Normal half range only (|x| >= 2^-14, 13 discarded bits); below it the
+    // subnormal spacing is fixed and round-to-nearest is kept.
+    __device__ static void store_sr(T* p, R v, int q, uint32_t r)
+    {
+        const float x = v * ShiftScale<L>::scale(q);
+        *p = fabsf(x) >= 6.103515625e-05f ? __float2half_rz(dither_bits(x, r, 13)) : __float2half_rn(x);
+    }
 };
 template <class L> struct StoreBF16 {
     static constexpr bool blocked = false;
+    static constexpr bool dither = true;
     using T = __nv_bfloat16;
     using R = float;
     static constexpr bool shifted = true;
     __device__ static R load(const T* p, int q, R) { return __bfloat162float(__ldg(p)) * ShiftScale<L>::inv(q); }
     __device__ static void store(T* p, R v, int q, R) { *p = __float2bfloat16_rn(v * ShiftScale<L>::scale(q)); }
+    __device__ static void store_sr(T* p, R v, int q, uint32_t r)
+    {
+        *p = __float2bfloat16_rz(dither_bits(v * ShiftScale<L>::scale(q), r, 16));
+    }
 };
 template <class L> struct StoreF32 {
     static constexpr bool blocked = false;
+    static constexpr bool dither = false;
     using T = float;
     using R = float;
     static constexpr bool shifted = true;
@@ -115,6 +141,7 @@ template <class L> struct StoreF32 {
 // Full (unshifted) populations in FP32 with FP32 arithmetic.
 struct StoreF32Full {
     static constexpr bool blocked = false;
+    static constexpr bool dither = false;
     using T = float;
     using R = float;
     static constexpr bool shifted = false;
@@ -134,6 +161,7 @@ template <class L> struct StoreBFP16 {
     using R = float;
     static constexpr bool shifted = true;
     static constexpr bool blocked = true;
+    static constexpr bool dither = false;
     static constexpr int kEmin = -100, kEmax = 100;
     __device__ static R load(const T*, int, R) { return R(0); }
     __device__ static void store(T*, R, int, R) {}
@@ -318,7 +346,17 @@ struct ScspParams {
     double inv_rho0;
     Trt rate;          // SRT: s+ = s- = 1/tau; MRT: legacy spectrum
     int mrt = 0;       // MRT: mass and momentum rows are not relaxed (rate 0)
+    uint32_t seed = 0; // non-zero: stochastic rounding of 16-bit float storage (per-step seed)
 };
+
+// Integer hash (lowbias32 of C. Wellons) seeding the per-node rounding stream.
+__device__ __forceinline__ uint32_t hash32(uint32_t x)
+{
+    x ^= x >> 16; x *= 0x7feb352du;
+    x ^= x >> 15; x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
 
 // Update of one fluid node i (the body of scsp_step, shared with the batched
 // kernel).
@@ -384,6 +422,20 @@ __device__ __forceinline__ void scsp_update(const Grid& g, const Force& F, const
 
     if constexpr (S::blocked) {
         S::store_blk(fout, g.nfp, i, f, eout);
+    } else if constexpr (S::dither) {
+        if (P.seed) {
+            // One linear congruential stream per node and step; its high bits
+            // are the rounding offsets.
+            uint32_t r = hash32(i * 0x9e3779b9u + P.seed);
+#pragma unroll
+            for (int q = 0; q < L::Q; ++q) {
+                r = r * 1664525u + 1013904223u;
+                S::store_sr(fout + (q * g.nfp + i), f[q], q, r);
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < L::Q; ++q) S::store(fout + (q * g.nfp + i), f[q], q, rho0);
+        }
     } else {
 #pragma unroll
         for (int q = 0; q < L::Q; ++q) S::store(fout + (q * g.nfp + i), f[q], q, rho0);
