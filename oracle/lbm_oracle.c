@@ -109,6 +109,7 @@ struct lbo_sim {
     double ai[2][QMAX], bi[QMAX];
     /* link classification */
     uint32_t *link;     /* bit (q-1): q-neighbour solid */
+    uint32_t *film[2];  /* bit (q-1): q-neighbour a half film (HF) of phase 0 / 1 */
     size_t *ibI;        /* 0 = not a wall node, else 1-based wall id */
     size_t nwall;
     double *ibSin, *ibCos, *tib, *tibInv, *ibNorm;  /* per wall id */
@@ -188,8 +189,8 @@ void lbo_mrt_tables(int q, double tau, double *m, double *minv, double *s)
 }
 
 /* Voxels that carry populations (the fluid sets of initialize, collision and
- * buildIb: VD, GV, PB, VB; HF is a color research selector, refused). */
-static int is_fluid_type(int t) { return t == LBO_VD || t == LBO_GV || t == LBO_PB || t == LBO_VB; }
+ * buildIb: VD, GV, PB, VB and, for the color model, HF). */
+static int is_fluid_type(int t) { return t == LBO_VD || t == LBO_GV || t == LBO_PB || t == LBO_VB || t == LBO_HF; }
 /* Voxels whose moments come from the populations (calcMacroVar's VD, GV). */
 static int is_bulk_type(int t) { return t == LBO_VD || t == LBO_GV; }
 static int is_solid_type(int t) { return t == LBO_BB || t == LBO_SD; }
@@ -235,6 +236,8 @@ static void build_ib(lbo_sim *s)
 {
     static const double pi = 3.1415926535897932384626433832795;
     s->link = calloc(s->N, sizeof(uint32_t));
+    s->film[0] = calloc(s->N, sizeof(uint32_t));
+    s->film[1] = calloc(s->N, sizeof(uint32_t));
     s->ibI = calloc(s->N, sizeof(size_t));
     size_t cap = 1024, c = 1;
     s->ibSin = malloc(cap * sizeof(double));
@@ -255,6 +258,8 @@ static void build_ib(lbo_sim *s)
                     for (int d = 0; d < s->D; ++d) norm[d] -= s->e[q][d];
                     ca += nb->value;
                     nCA++;
+                } else if (nb->type == LBO_HF) {   /* half permeable film (simulator.cpp:418-421) */
+                    s->film[nb->phase][i] |= 1u << (q - 1);
                 }
             }
             if (isIB) {
@@ -339,6 +344,8 @@ lbo_sim *lbo_create(const lbo_params *p, const lbo_label labels[256], const uint
         const lbo_label *l = &labels[geometry[i]];
         int t = l->type;
         if (!is_fluid_type(t) && !is_solid_type(t)) { free(s); return NULL; }
+        /* Half films are a two-phase label (ColorFluid::clearHalfFilm). */
+        if (t == LBO_HF && (!p->color || l->phase < 0 || l->phase > 1)) { free(s); return NULL; }
         /* FilePrm checks (fileprm.cpp:280-289). */
         if (t == LBO_PB || t == LBO_VB) {
             if (l->dir < 1 || l->dir > 2 * s->D || !isfinite(l->value) ||
@@ -410,7 +417,7 @@ void lbo_destroy(lbo_sim *s)
     free(s->geom); free(s->f); free(s->fold);
     free(s->dens[0]); free(s->dens[1]); free(s->densT); free(s->densN); free(s->tau);
     for (int d = 0; d < 3; ++d) free(s->v[d]);
-    free(s->link); free(s->ibI); free(s->ibSin); free(s->ibCos); free(s->ibNorm);
+    free(s->link); free(s->film[0]); free(s->film[1]); free(s->ibI); free(s->ibSin); free(s->ibCos); free(s->ibNorm);
     free(s->tib); free(s->tibInv);
     free(s);
 }
@@ -877,6 +884,23 @@ static void stream_bounce(lbo_sim *s)
             for (size_t i = 0; i < s->N; ++i)
                 if (s->link[i] & (1u << (q - 1))) F(ph, opq, i) = FO(ph, q, i);
         }
+    if (s->phases == 2) {
+        /* ColorFluid::Run (colorfluid.cpp:155-158): phase 0 bounces back from
+         * films of phase 1 and phase 1 from films of phase 0; then
+         * clearHalfFilm (colorfluid.cpp:752-765) empties the other phase at
+         * every film voxel. */
+        for (int ph = 0; ph < 2; ++ph)
+            for (int q = 1; q < s->Q; ++q) {
+                const int opq = s->op[q];
+                for (size_t i = 0; i < s->N; ++i)
+                    if (s->film[1 - ph][i] & (1u << (q - 1))) F(ph, opq, i) = FO(ph, q, i);
+            }
+        for (size_t i = 0; i < s->N; ++i) {
+            const lbo_label *l = &s->lab[s->geom[i]];
+            if (l->type != LBO_HF) continue;
+            for (int q = 0; q < s->Q; ++q) F(1 - l->phase, q, i) = 0;
+        }
+    }
 }
 
 int lbo_initialize(lbo_sim *s)

@@ -226,6 +226,43 @@ def color_zou_he_cases():
     return out
 
 
+def film_cases():
+    """Half-permeable films (HF; simulator.cpp:418-421, colorfluid.cpp:155-158,
+    752-765): a film voxel lets its own phase through and bounces the other
+    back, and holds only its own phase.  A D2Q9 channel driven by GV forces
+    through a phase-0 film, and a D3Q19 tube after the reference's HalfFilm
+    sample: a film of each phase across the inlet side, VB inlets per phase,
+    a PB outlet, unequal densities and viscosities."""
+    nx, ny = 24, 12
+    g = np.full((ny, nx), 0, np.uint8)
+    g[:, nx // 2:] = 100
+    g[:, 8:10] = 25
+    g[0, :] = 255
+    g[-1, :] = 255
+    d2 = dict(name='film-d2-MRT', geometry=g,
+              labels={0: ('GV', 2e-5, 1, 0), 100: ('GV', 2e-5, 1, 1), 25: ('HF', 0, 0, 0),
+                      255: ('SD', 90.0, 0, 0)},
+              model='color', collision='MRT', tau=(1.0, 0.8), rho=(1.0, 1.0), alpha0=4 / 9,
+              sigma=5e-3, beta=0.7, steps=300, write=300)
+    nx, ny, nz = 8, 6, 24
+    g = np.full((nz, ny, nx), 0, np.uint8)
+    g[:, :, nx // 2:] = 100
+    g[0, :, :nx // 2] = 50
+    g[0, :, nx // 2:] = 150
+    g[3:5, :, :nx // 2] = 25
+    g[3:5, :, nx // 2:] = 125
+    g[-1] = 200
+    g[:, 0, :] = 255
+    g[:, -1, :] = 255
+    d3 = dict(name='film-d3-MRT', geometry=g,
+              labels={0: ('VD', 0, 0, 0), 25: ('HF', 0, 0, 0), 50: ('VB', 1e-3, 5, 0),
+                      100: ('VD', 0, 0, 1), 125: ('HF', 0, 0, 1), 150: ('VB', 1e-3, 5, 1),
+                      200: ('PB', 1.0, 6, 0), 255: ('SD', 90.0, 0, 0)},
+              model='color', collision='MRT', tau=(0.57, 1.2154), rho=(1.0, 0.831683168), alpha0=1 / 3,
+              sigma=0.0859, beta=0.7, steps=200, write=200)
+    return [d2, d3]
+
+
 def pressure_report_channel():
     """scripts/porous_media.py:257-279 (pressure_study): a 16-wide slit between
     SD walls, PB inlet 1 + 3e-5 and outlet 1 along x, MRT tau 1, 6000 steps,
@@ -250,7 +287,7 @@ def golden_cases():
     return ([channel_config1(), channel_mrt(), drop_3d(), wall_color_3d(0.7, 'MRT'),
              wall_color_3d(1.0, 'SRT'), wall_color_2d('MRT'), wall_color_2d('SRT'),
              porous_scsp('MRT'), porous_scsp('SRT'), porous_scsp_2d('MRT')] + force_cases()
-            + zou_he_cases() + color_zou_he_cases())
+            + zou_he_cases() + color_zou_he_cases() + film_cases())
 
 
 def prm_text(case, grid_file='geometry.raw', out='field', report_dir=0):
@@ -281,7 +318,7 @@ def prm_text(case, grid_file='geometry.raw', out='field', report_dir=0):
     for k, (t, v, d, ph) in sorted(case['labels'].items()):
         val = 'N/A' if t in ('VD', 'BB') else format(v, '.17g') if t in ('GV', 'PB', 'VB') else format(v, 'g')
         dr = str(d) if t in ('GV', 'PB', 'VB') else 'N/A'
-        p = str(ph) if t in ('VD', 'GV', 'PB', 'VB') else 'N/A'
+        p = str(ph) if t in ('VD', 'GV', 'PB', 'VB', 'HF') else 'N/A'
         lines.append(f'{k} "{t}" "{val}" "{dr}" "{p}"')
     if not color:
         pass
