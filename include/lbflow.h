@@ -82,7 +82,8 @@ typedef struct {
     int32_t dir;      /* GV: lattice direction of the force; PB/VB: the axial
                          direction 1..2*dims pointing into the domain (the
                          direction of the populations the boundary rebuilds) */
-    int32_t phase;    /* VD/GV/PB/VB: fluid phase */
+    int32_t phase;    /* VD/GV/PB/VB: fluid phase; HF: the phase the film
+                         lets through (color model only) */
     int32_t reserved;
     double value;     /* GV: force magnitude; PB: density; VB: speed along dir
                          (SCSP::zouHeBoundary, scsp.cpp:188-275;

@@ -30,6 +30,60 @@ struct ColorWall {
 
 constexpr double kSolidPhi = 86.0;
 
+// Half-permeable films (HF voxels): bits[k] marks the film voxels of phase k
+// in the occupancy map's word layout (nullptr when the geometry has none).
+struct Film {
+    const uint32_t* __restrict__ bits[2];
+};
+
+// Bit q set when the pull source x - e_q is a film voxel of the bitmap.
+template <class L>
+__device__ __forceinline__ uint32_t film_sources(const Grid& g, const uint32_t* __restrict__ bits, int x, int y, int z)
+{
+    uint32_t m = 0;
+#pragma unroll
+    for (int q = 1; q < L::Q; ++q) {
+        const int sx = wrap(x - L::ex(q), g.nx), sy = wrap(y - L::ey(q), g.ny);
+        const int sz = L::D == 3 ? wrap(z - L::ez(q), g.nz) : 0;
+        const uint32_t w = __ldg(&bits[((size_t)sz * g.ny + sy) * g.W + (sx >> 5)]);
+        m |= ((w >> (sx & 31)) & 1u) << q;
+    }
+    return m;
+}
+
+// Both components' incoming populations of node i.  With films (FILM, pull
+// steps only): phase 0 bounces back from films of phase 1 and phase 1 from
+// films of phase 0 (ColorFluid::Run, colorfluid.cpp:155-158), then a film
+// voxel keeps only its own phase (clearHalfFilm, colorfluid.cpp:752-765).
+// nbr keeps the occupancy neighbours: a film voxel is fluid for the gradient.
+template <class L, class S, bool PULL, bool FILM>
+__device__ __forceinline__ void color_gather(const Grid& g, const Film& film, const typename S::T* __restrict__ fin,
+                                             uint32_t i, int x, int y, int z, typename S::R (&f0)[L::Q],
+                                             typename S::R (&f1)[L::Q], uint32_t (&nbr)[L::Q])
+{
+    using R = typename S::R;
+    gather<L, S, PULL>(g, fin, i, x, y, z, f0, nbr, R(0));
+    gather<L, S, PULL>(g, fin + (size_t)L::Q * g.nfp, i, x, y, z, f1, nbr, R(0));
+    if constexpr (FILM && PULL) {
+        const uint32_t b1 = film_sources<L>(g, film.bits[1], x, y, z);   // blocks phase 0
+        const uint32_t b0 = film_sources<L>(g, film.bits[0], x, y, z);   // blocks phase 1
+        const typename S::T* in1 = fin + (size_t)L::Q * g.nfp;
+#pragma unroll
+        for (int q = 1; q < L::Q; ++q) {
+            if ((b1 >> q) & 1u) f0[q] = S::load(fin + ((size_t)L::op(q) * g.nfp + i), L::op(q), R(0));
+            if ((b0 >> q) & 1u) f1[q] = S::load(in1 + ((size_t)L::op(q) * g.nfp + i), L::op(q), R(0));
+        }
+        const size_t w = ((size_t)z * g.ny + y) * g.W + (x >> 5);
+        const uint32_t own0 = (__ldg(&film.bits[0][w]) >> (x & 31)) & 1u;
+        const uint32_t own1 = (__ldg(&film.bits[1][w]) >> (x & 31)) & 1u;
+#pragma unroll
+        for (int q = 0; q < L::Q; ++q) {
+            if (own0) f1[q] = R(0);
+            if (own1) f0[q] = R(0);
+        }
+    }
+}
+
 // Non-contracted IEEE arithmetic (never fused into FMA).
 __device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
@@ -48,9 +102,9 @@ template <class L> __host__ __device__ inline int normal_code(int n0, int n1, in
 template <class L> constexpr int normal_codes() { return L::D == 3 ? 11 * 11 * 11 : 7 * 7; }
 
 // Pass 1: phase field.  PULL = false reads the node's own values (t = 0).
-template <class L, class S, bool PULL>
+template <class L, class S, bool PULL, bool FILM>
 __global__ void __launch_bounds__(128)
-color_phase(const Grid g, const typename S::T* __restrict__ fin, double* __restrict__ phi,
+color_phase(const Grid g, const Film film, const typename S::T* __restrict__ fin, double* __restrict__ phi,
             uint32_t* __restrict__ err)
 {
     using R = typename S::R;
@@ -60,8 +114,7 @@ color_phase(const Grid g, const typename S::T* __restrict__ fin, double* __restr
     unpack(__ldg(&g.coord[i]), x, y, z);
     R f0[L::Q], f1[L::Q];
     uint32_t nbr[L::Q];
-    gather<L, S, PULL>(g, fin, i, x, y, z, f0, nbr, R(0));
-    gather<L, S, PULL>(g, fin + (size_t)L::Q * g.nfp, i, x, y, z, f1, nbr, R(0));
+    color_gather<L, S, PULL, FILM>(g, film, fin, i, x, y, z, f0, f1, nbr);
     R d0 = f0[0], d1 = f1[0];
 #pragma unroll
     for (int q = 1; q < L::Q; ++q) { d0 += f0[q]; d1 += f1[q]; }
@@ -280,9 +333,9 @@ __device__ __forceinline__ void color_update(const Grid& g, const Force& F, cons
 
 // Pass 2: collision, gradient, perturbation and recoloring of every fluid node.
 // PULL = false is the t = 0 collision.
-template <class L, class S, int COLL, bool PULL>
+template <class L, class S, int COLL, bool PULL, bool FILM>
 __global__ void __launch_bounds__(128)
-color_collide(const Grid g, const Force F, const ColorParams P, const ColorWall W,
+color_collide(const Grid g, const Film film, const Force F, const ColorParams P, const ColorWall W,
               const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
               const double* __restrict__ phi, Macros mo, const int out, uint32_t* __restrict__ err)
 {
@@ -293,8 +346,7 @@ color_collide(const Grid g, const Force F, const ColorParams P, const ColorWall 
     unpack(__ldg(&g.coord[i]), x, y, z);
     R f0[L::Q], f1[L::Q];
     uint32_t nbr[L::Q];
-    gather<L, S, PULL>(g, fin, i, x, y, z, f0, nbr, R(0));
-    gather<L, S, PULL>(g, fin + (size_t)L::Q * g.nfp, i, x, y, z, f1, nbr, R(0));
+    color_gather<L, S, PULL, FILM>(g, film, fin, i, x, y, z, f0, f1, nbr);
     if (!PULL) {
         // t = 0: neighbours by direct lookup (the pull above read local values).
 #pragma unroll
@@ -372,8 +424,8 @@ __device__ __forceinline__ void color_zou_he_node(R (&f0)[L::Q], R (&f1)[L::Q], 
 
 // Gather a boundary node and apply the rule; returns the boundary density and
 // axial velocity (ua on axis *axis).
-template <class L, class S>
-__device__ __forceinline__ void color_zou_he_gather(const Grid& g, const ZouHe& z, const uint32_t k,
+template <class L, class S, bool FILM>
+__device__ __forceinline__ void color_zou_he_gather(const Grid& g, const Film& film, const ZouHe& z, const uint32_t k,
                                                     const typename S::T* __restrict__ fin, uint32_t& i,
                                                     typename S::R (&f0)[L::Q], typename S::R (&f1)[L::Q],
                                                     uint32_t (&nbr)[L::Q], typename S::R& dens,
@@ -384,8 +436,7 @@ __device__ __forceinline__ void color_zou_he_gather(const Grid& g, const ZouHe& 
     const double val = __ldg(&z.value[k]);
     int x, y, zc;
     unpack(__ldg(&g.coord[i]), x, y, zc);
-    gather<L, S, true>(g, fin, i, x, y, zc, f0, nbr, typename S::R(0));
-    gather<L, S, true>(g, fin + (size_t)L::Q * g.nfp, i, x, y, zc, f1, nbr, typename S::R(0));
+    color_gather<L, S, true, FILM>(g, film, fin, i, x, y, zc, f0, f1, nbr);
     const uint32_t kind = (code >> 8) & 0xffu;
     const int phs = (int)(code >> 16);
     const int dir = (int)(code & 0xffu);
@@ -405,9 +456,9 @@ __device__ __forceinline__ void color_zou_he_gather(const Grid& g, const ZouHe& 
 }
 
 // Boundary phase pass: phi of the boundary nodes from their rebuilt populations.
-template <class L, class S>
+template <class L, class S, bool FILM>
 __global__ void __launch_bounds__(128)
-color_zou_he_phase(const Grid g, const ZouHe z, const typename S::T* __restrict__ fin,
+color_zou_he_phase(const Grid g, const Film film, const ZouHe z, const typename S::T* __restrict__ fin,
                    double* __restrict__ phi, uint32_t* __restrict__ err)
 {
     using R = typename S::R;
@@ -417,7 +468,7 @@ color_zou_he_phase(const Grid g, const ZouHe z, const typename S::T* __restrict_
     R f0[L::Q], f1[L::Q], dens, ua;
     uint32_t nbr[L::Q];
     int axis;
-    color_zou_he_gather<L, S>(g, z, k, fin, i, f0, f1, nbr, dens, ua, axis);
+    color_zou_he_gather<L, S, FILM>(g, film, z, k, fin, i, f0, f1, nbr, dens, ua, axis);
     R d0 = f0[0], d1 = f1[0];
 #pragma unroll
     for (int q = 1; q < L::Q; ++q) { d0 += f0[q]; d1 += f1[q]; }
@@ -431,9 +482,10 @@ color_zou_he_phase(const Grid g, const ZouHe z, const typename S::T* __restrict_
 // Boundary collision pass (after pass 2); also keeps the report's adjacent
 // history of the boundary nodes as the reference forms it.  z.num[k] holds
 // rho0 - rho1 of the last step that asked for the adjacent history.
-template <class L, class S, int COLL>
+template <class L, class S, int COLL, bool FILM>
 __global__ void __launch_bounds__(128)
-color_zou_he_collide(const Grid g, const Force F, const ColorParams P, const ColorWall W, const ZouHe z,
+color_zou_he_collide(const Grid g, const Film film, const Force F, const ColorParams P, const ColorWall W,
+                     const ZouHe z,
                      const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
                      const double* __restrict__ phi, Macros mo, const int out, uint32_t* __restrict__ err)
 {
@@ -444,7 +496,7 @@ color_zou_he_collide(const Grid g, const Force F, const ColorParams P, const Col
     R f0[L::Q], f1[L::Q], dens, ua;
     uint32_t nbr[L::Q];
     int axis;
-    color_zou_he_gather<L, S>(g, z, k, fin, i, f0, f1, nbr, dens, ua, axis);
+    color_zou_he_gather<L, S, FILM>(g, film, z, k, fin, i, f0, f1, nbr, dens, ua, axis);
     R d0 = f0[0], d1 = f1[0];
 #pragma unroll
     for (int q = 1; q < L::Q; ++q) { d0 += f0[q]; d1 += f1[q]; }

@@ -5,8 +5,8 @@
 namespace lbf {
 
 namespace {
-template <class L, class S, int COLL>
-void dispatch(bool pull, int out, const ColorLaunch& a)
+template <class L, class S, int COLL, bool FILM>
+void run_step(bool pull, int out, const ColorLaunch& a)
 {
     using T = typename S::T;
     const T* fin = static_cast<const T*>(a.fin);
@@ -14,22 +14,30 @@ void dispatch(bool pull, int out, const ColorLaunch& a)
     const unsigned threads = 128, blocks = blocks_for(a.g.nf, threads);
     if (blocks == 0) return;
     const unsigned zb = blocks_for(a.zh.n, threads);
-    if (pull) color_phase<L, S, true><<<blocks, threads, 0, a.stream>>>(a.g, fin, a.phi, a.err);
-    else color_phase<L, S, false><<<blocks, threads, 0, a.stream>>>(a.g, fin, a.phi, a.err);
+    if (pull) color_phase<L, S, true, FILM><<<blocks, threads, 0, a.stream>>>(a.g, a.film, fin, a.phi, a.err);
+    else color_phase<L, S, false, false><<<blocks, threads, 0, a.stream>>>(a.g, a.film, fin, a.phi, a.err);
     // Zou-He boundary nodes (PB/VB): their phase from the rebuilt populations
     // before pass 2 reads it, and their collision after pass 2 (overwriting).
-    if (pull && zb) color_zou_he_phase<L, S><<<zb, threads, 0, a.stream>>>(a.g, a.zh, fin, a.phi, a.err);
+    if (pull && zb)
+        color_zou_he_phase<L, S, FILM><<<zb, threads, 0, a.stream>>>(a.g, a.film, a.zh, fin, a.phi, a.err);
     if (!pull && zb && (out & kOutAdjacent)) color_zou_he_record<L, S><<<zb, threads, 0, a.stream>>>(a.g, a.zh, fin);
     if (pull)
-        color_collide<L, S, COLL, true><<<blocks, threads, 0, a.stream>>>(
-            a.g, a.F, a.P, a.W, fin, fout, a.phi, a.mo, out, a.err);
+        color_collide<L, S, COLL, true, FILM><<<blocks, threads, 0, a.stream>>>(
+            a.g, a.film, a.F, a.P, a.W, fin, fout, a.phi, a.mo, out, a.err);
     else
-        color_collide<L, S, COLL, false><<<blocks, threads, 0, a.stream>>>(
-            a.g, a.F, a.P, a.W, fin, fout, a.phi, a.mo, out, a.err);
+        color_collide<L, S, COLL, false, false><<<blocks, threads, 0, a.stream>>>(
+            a.g, a.film, a.F, a.P, a.W, fin, fout, a.phi, a.mo, out, a.err);
     if (pull && zb)
-        color_zou_he_collide<L, S, COLL><<<zb, threads, 0, a.stream>>>(a.g, a.F, a.P, a.W, a.zh, fin, fout,
-                                                                      a.phi, a.mo, out, a.err);
+        color_zou_he_collide<L, S, COLL, FILM><<<zb, threads, 0, a.stream>>>(a.g, a.film, a.F, a.P, a.W, a.zh, fin,
+                                                                            fout, a.phi, a.mo, out, a.err);
+}
 
+template <class L, class S, int COLL>
+void dispatch(bool pull, int out, const ColorLaunch& a)
+{
+    // Half films: the film-aware gathers only where the geometry has films.
+    if (a.film.bits[0]) run_step<L, S, COLL, true>(pull, out, a);
+    else run_step<L, S, COLL, false>(pull, out, a);
 }
 
 template <class L, class S>

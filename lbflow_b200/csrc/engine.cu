@@ -46,6 +46,7 @@ struct lbf_engine {
     ZouHe zh{};                     // PB/VB boundary nodes (single phase)
     uint32_t *zh_node = nullptr, *zh_code = nullptr;
     double *zh_value = nullptr, *zh_num = nullptr;
+    uint32_t* film_bits[2] = {nullptr, nullptr};   // half-film voxels of phase 0 / 1 (color)
     ScspParams sp{};
     ColorParams cp{};
     bool initialized = false;
@@ -96,7 +97,7 @@ const int kE19[19][3] = {{0,0,0},{0,0,1},{0,0,-1},{0,1,0},{0,-1,0},{1,0,0},{-1,0
 // collision and Simulator::buildIb (scsp.cpp:116-134, 374-464;
 // simulator.cpp:399-415; ColorFluid's initialize / calcMacroVar / collision
 // sets, colorfluid.cpp:220, 244, 323).
-bool is_fluid(int t) { return t == LBF_VD || t == LBF_GV || t == LBF_PB || t == LBF_VB; }
+bool is_fluid(int t) { return t == LBF_VD || t == LBF_GV || t == LBF_PB || t == LBF_VB || t == LBF_HF; }
 bool is_solid(int t) { return t == LBF_BB || t == LBF_SD; }
 
 // e_q component a (0 = x, 1 = y, 2 = z) of the reference tables.
@@ -189,7 +190,8 @@ void launch_step(lbf_engine* e, bool pull, int out)
         if (pull && e->zh.n) launch_scsp_zou_he(e->D, (int)e->cfg.storage, a, e->zh);
     } else {
         ColorWall W{e->angle_id, e->angles, e->tib};
-        ColorLaunch a{grid_of(e), e->force, e->cp, W, fin, fout, e->phi, macros_of(e), e->err, e->stream, e->zh};
+        ColorLaunch a{grid_of(e), e->force, e->cp, W, fin, fout, e->phi, macros_of(e), e->err, e->stream, e->zh,
+                      Film{{e->film_bits[0], e->film_bits[1]}}};
         launch_color(e->D, (int)e->cfg.storage, (int)e->cfg.collision, pull, out, a);
     }
     e->cur ^= 1;
@@ -471,7 +473,9 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
         const lbf_label& L = labels[l];
         if (L.type == 0) return bail(LBF_EINVAL, "geometry label " + std::to_string(l) + " is not defined");
         if (!is_fluid(L.type) && !is_solid(L.type))
-            return bail(LBF_EINVAL, "label " + std::to_string(l) + ": only VD, GV, PB, VB, BB and SD labels are supported");
+            return bail(LBF_EINVAL, "label " + std::to_string(l) + ": only VD, GV, PB, VB, HF, BB and SD labels are supported");
+        if (L.type == LBF_HF && c.model != LBF_MODEL_COLOR)
+            return bail(LBF_EINVAL, "label " + std::to_string(l) + ": half-permeable films (HF) need the color model");
         if ((L.type == LBF_PB || L.type == LBF_VB) && !std::isfinite(L.value))
             return bail(LBF_EINVAL, "Non-finite boundary value.");
         if ((L.type == LBF_PB || L.type == LBF_VB) && (L.dir <= 0 || L.dir >= e->Q))
@@ -590,6 +594,23 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
     LBF_CUDA(cudaMemcpyAsync(e->occ, occ.data(), occ.size() * sizeof(uint2), cudaMemcpyHostToDevice, e->stream));
     LBF_CUDA(cudaMemcpyAsync(e->coord, coord.data(), coord.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, e->stream));
     LBF_CUDA(cudaMemcpyAsync(e->label_force, lforce.data(), lforce.size() * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+    // Half-film bitmaps in the occupancy word layout (simulator.cpp:418-421).
+    bool films = false;
+    for (int l = 0; l < 256; ++l) films |= used[l] && labels[l].type == LBF_HF;
+    if (films) {
+        std::vector<uint32_t> fb[2] = {std::vector<uint32_t>(rows * e->W, 0u), std::vector<uint32_t>(rows * e->W, 0u)};
+        for (size_t v = 0; v < e->N; ++v) {
+            const lbf_label& L = labels[geometry[v]];
+            if (L.type != LBF_HF) continue;
+            const size_t r = v / e->nx, x = v % e->nx;
+            fb[L.phase][r * e->W + (x >> 5)] |= 1u << (x & 31);
+        }
+        for (int k = 0; k < 2; ++k) {
+            LBF_ALLOC(e->film_bits[k], fb[k].size());
+            LBF_CUDA(cudaMemcpyAsync(e->film_bits[k], fb[k].data(), fb[k].size() * sizeof(uint32_t),
+                                     cudaMemcpyHostToDevice, e->stream));
+        }
+    }
     if (!zh_node.empty()) {
         LBF_ALLOC(e->zh_node, zh_node.size());
         LBF_ALLOC(e->zh_code, zh_code.size());
@@ -741,7 +762,7 @@ void lbf_destroy(lbf_engine* e)
     void* ptrs[] = {e->f[0], e->f[1], e->ex[0], e->ex[1], e->occ, e->coord, e->node_label, e->node_phase, e->label_force,
                     e->rho0, e->rho1, e->u, e->uprev, e->uadj, e->ind, e->indprev, e->indadj,
                     e->phi, e->angle_id, e->angles, e->tib, e->err, e->partial, e->red,
-                    e->zh_node, e->zh_code, e->zh_value, e->zh_num, e->dense_tmp};
+                    e->zh_node, e->zh_code, e->zh_value, e->zh_num, e->dense_tmp, e->film_bits[0], e->film_bits[1]};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (e->h_red) cudaFreeHost(e->h_red);
     if (e->stream) cudaStreamDestroy(e->stream);

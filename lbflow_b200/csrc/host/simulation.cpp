@@ -98,11 +98,6 @@ Simulation::Simulation(const Params& p) : p_(p)
     }
     if (!color_ && p.equilModel() != "SRT" && p.equilModel() != "MRT")
         throw std::invalid_argument("Invalid equilibrium model.");
-    for (int v = 0; v < 256; ++v) {
-        if (!used[v]) continue;
-        const LabelType t = p.label(v).type;
-        if (t == HF) throw std::invalid_argument("Half-permeable films (HF) are not supported by the B200 engine.");
-    }
     // fluid_nodes of the timing line (simulator.cpp:47-56).
     for (uint8_t v : geometry_) {
         const LabelType t = p.label(v).type;

@@ -34,6 +34,7 @@ struct ColorLaunch {
     uint32_t* err;
     cudaStream_t stream;
     ZouHe zh;          // PB/VB boundary nodes (n = 0: none)
+    Film film;         // half-permeable film bitmaps (nullptr: none)
 };
 
 // storage: LBF_STORE_* value; dims: 2 or 3.

@@ -23,6 +23,6 @@ def fluid_mask(case):
     g = np.asarray(case['geometry'])
     fl = np.zeros(g.shape, bool)
     for k, (t, *_rest) in case['labels'].items():
-        if TYPES[t] in (0x1, 0x2, 0x4, 0x8):      # VD, GV, PB, VB carry populations
+        if TYPES[t] in (0x1, 0x2, 0x4, 0x8, 0x40):   # VD, GV, PB, VB, HF carry populations
             fl |= g == k
     return fl

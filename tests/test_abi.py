@@ -45,7 +45,8 @@ def _create(**over):
     (dict(collision=5), 'collision'),
     (dict(tau=(0.5, 1.0)), 'relaxation times must exceed 0.5'),
     (dict(labels={}), 'not defined'),
-    (dict(labels={0: ('HF', 0.0, 0, 0)}), 'only VD, GV, PB, VB, BB and SD'),
+    (dict(labels={0: ('HF', 0.0, 0, 0)}), 'half-permeable films (HF) need the color model'),
+    (dict(labels={0: ('AB', 0.0, 0, 0)}), 'only VD, GV, PB, VB, HF, BB and SD'),
     (dict(model=1, labels={0: ('PB', 1.0, 1, 2)}), 'phase'),
     (dict(labels={0: ('PB', 0.0, 1, 0)}), 'Pressure-boundary density must be positive'),
     (dict(labels={0: ('VB', 1e-3, 7, 0)}), 'axial direction'),
