@@ -476,22 +476,44 @@ def batch_geometries(count, seed=2024):
 def batch_run(args):
     """All geometries in one batch, each converged to the 1e-6 criterion and
     retired; aggregate fluid MLUPS; permeability of a sample re-solved alone
-    with the plain FP64 engine."""
+    with the plain FP64 engine.  Under torchrun the geometries are split over
+    the ranks (one GPU each, batch.converge_sharded): no data-path
+    collective, the per-geometry results gathered host-side over gloo, the
+    time the slowest rank's."""
     import torch
     from lbflow_b200 import Engine
-    from lbflow_b200.batch import Batch
+    from lbflow_b200.batch import Batch, converge_sharded
     from lbflow_b200.permeability import converge
-    torch.cuda.set_device(0)
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group('gloo', timeout=timedelta(seconds=600))
     t0 = time.perf_counter()
     geoms, taus, specs = batch_geometries(args.count)
     gen_s = time.perf_counter() - t0
     storage = args.storage if args.storage in ('fp64', 'fp32', 'fp16') else 'fp64'
-    b = Batch(geoms, taus, LABELS, collision=args.collision, storage=storage)
-    b.initialize()
-    tune = b.autotune(steps=6)
-    res = b.converge(1e-5, report=1000, tol=1e-6, max_steps=args.max_steps)
-    nodes = b.fluid_nodes()
-    b.close()
+    tune = None
+    if world > 1:
+        dist.barrier()
+        res = converge_sharded(geoms, taus, LABELS, 1e-5, rank=rank, world=world, device=local,
+                               collision=args.collision, storage=storage, report=1000, tol=1e-6,
+                               max_steps=args.max_steps)
+        nodes = res['nodes']
+        dist.barrier()
+        dist.destroy_process_group()
+        if rank != 0:
+            return 0
+    else:
+        b = Batch(geoms, taus, LABELS, collision=args.collision, storage=storage)
+        b.initialize()
+        tune = b.autotune(steps=6)
+        res = b.converge(1e-5, report=1000, tol=1e-6, max_steps=args.max_steps)
+        nodes = b.fluid_nodes()
+        b.close()
     check = []
     for k in range(min(args.check, args.count)):
         e = Engine(geoms[k], LABELS, collision=args.collision, tau=(taus[k],))
@@ -500,7 +522,8 @@ def batch_run(args):
         check.append(dict(geometry=k, shape=list(specs[k][0]), K_batch=float(res['K'][k]), K_fp64=r['K'],
                           rel_error=abs(res['K'][k] - r['K']) / abs(r['K']), steps=int(res['steps'][k])))
     print(json.dumps(dict(metric='batched D3Q19 MRT aggregate fluid MLUPS',
-                          value=res['mlups'], unit='MLUPS', geometries=args.count, fluid_nodes=nodes,
+                          value=res['mlups'], unit='MLUPS', n_gpus=world,
+                          scaling='strong' if world > 1 else None, geometries=args.count, fluid_nodes=nodes,
                           converged=int(res['converged'].sum()), seconds=res['seconds'],
                           steps_max=int(res['steps'].max()), dtype=storage, autotune=tune,
                           generation_seconds=gen_s, permeability_check=check,

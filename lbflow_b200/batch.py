@@ -197,3 +197,82 @@ class Batch:
         seconds = time.perf_counter() - t0
         return dict(steps=steps, K=K, converged=stable >= 3, seconds=seconds, updates=updates,
                     mlups=updates / seconds / 1e6)
+
+
+# ---- several GPUs: the batch split into independent shards -------------------
+def estimated_work(geometries, taus, labels):
+    """Relative cost of converging each geometry: fluid voxels times steps,
+    the steps scaling as the viscous time across the medium, L^2 / nu with L
+    the longest edge (the slow pressure mode crosses the whole medium)."""
+    from . import LABEL_TYPES
+    fluid_types = {LABEL_TYPES[t] for t in ('VD', 'GV', 'PB', 'VB')}
+    lut = np.zeros(256, bool)
+    for k, (t, *_rest) in labels.items():
+        lut[int(k)] = (LABEL_TYPES[t] if isinstance(t, str) else int(t)) in fluid_types
+    work = []
+    for g, tau in zip(geometries, taus):
+        nf = int(lut[np.asarray(g, np.uint8)].sum())
+        nu = (float(tau) - 0.5) / 3.0
+        work.append(nf * max(g.shape) ** 2 / nu)
+    return work
+
+
+def partition(work, parts):
+    """Longest-processing-time split of items with the given work into
+    `parts` lists of indices: items in order of decreasing work, each to the
+    currently lightest part (ties to the lower index, so every process that
+    calls this with the same work gets the same split).  Each list is
+    returned in ascending index order."""
+    order = sorted(range(len(work)), key=lambda k: (-work[k], k))
+    load = [0.0] * parts
+    out = [[] for _ in range(parts)]
+    for k in order:
+        p = min(range(parts), key=lambda j: (load[j], j))
+        out[p].append(k)
+        load[p] += work[k]
+    return [sorted(o) for o in out]
+
+
+def converge_sharded(geometries, taus, labels, g, rank=0, world=1, device=0, collision='MRT', storage='fp64',
+                     report=1000, tol=1e-6, max_steps=200000, group=None, batch_factory=None):
+    """Converge a list of geometries split over `world` processes, one GPU
+    each.  Geometries are independent, so there is no data-path collective:
+    every rank runs its share (partition of estimated_work) in its own
+    persistent batched launch, and only the per-geometry results (steps, K,
+    convergence flag) and each rank's seconds are exchanged afterwards,
+    host-side, with torch.distributed.all_gather_object on `group`.
+    Returns the results in the original order, seconds = the slowest rank's
+    wall time, and the aggregate node updates."""
+    factory = batch_factory or Batch
+    parts = partition(estimated_work(geometries, taus, labels), world)
+    mine = parts[rank]
+    local = dict(index=mine, steps=[], K=[], converged=[], seconds=0.0, updates=0, nodes=0)
+    if mine:
+        b = factory([geometries[k] for k in mine], [taus[k] for k in mine], labels, collision=collision,
+                    storage=storage, device=device)
+        try:
+            r = b.converge(g, report=report, tol=tol, max_steps=max_steps)
+            local.update(steps=[int(v) for v in r['steps']], K=[float(v) for v in r['K']],
+                         converged=[bool(v) for v in r['converged']], seconds=float(r['seconds']),
+                         updates=int(r['updates']), nodes=int(b.fluid_nodes()))
+        finally:
+            b.close()
+    if world > 1:
+        import torch.distributed as dist
+        gathered = [None] * world
+        dist.all_gather_object(gathered, local, group=group)
+    else:
+        gathered = [local]
+    n = len(geometries)
+    K = np.full(n, np.nan)
+    steps = np.zeros(n, int)
+    converged = np.zeros(n, bool)
+    for part in gathered:
+        for j, k in enumerate(part['index']):
+            K[k], steps[k], converged[k] = part['K'][j], part['steps'][j], part['converged'][j]
+    seconds = max(p['seconds'] for p in gathered)
+    updates = sum(p['updates'] for p in gathered)
+    return dict(K=K, steps=steps, converged=converged, seconds=seconds, updates=updates,
+                mlups=updates / seconds / 1e6 if seconds > 0 else 0.0,
+                nodes=sum(p['nodes'] for p in gathered), parts=[p['index'] for p in gathered],
+                rank_seconds=[p['seconds'] for p in gathered])
