@@ -299,14 +299,17 @@ const char *lbf_batch_last_error(const lbf_batch *b);
  * the device, for callers that cannot allocate device memory (a frozen or
  * exhausted memory pool, an allocator that owns the whole device).  Nothing
  * is allocated: the per-tile partial sums live in a fixed scratch array
- * compiled into the library (1,179,648 bytes, held on every GPU that loads
- * the library until exit).  No counterpart in the reference.
+ * compiled into the library (1,179,648 bytes), which comes into a device's
+ * memory with the library's module -- under CUDA's default lazy module
+ * loading at the first call on that device -- and stays until exit.  No
+ * counterpart in the reference.
  *   u:    [3][stride] x, y, z velocities;  rho0, rho1: [stride] densities
  *         (rho1 NULL for single phase);  n <= 16,777,216 nodes, else
  *         LBF_EINVAL;  out: 9 doubles in device memory, same order as
  *         lbf_flux_sums;  stream: a cudaStream_t (NULL = default stream).
- * The first call on a device looks up the scratch address and must come
- * before any stream capture.  Calls share the scratch: calls whose GPU work
+ * The first call on a device looks up the scratch address (and loads the
+ * module with its scratch): make it, n = 0 is enough, while device memory is
+ * still free and before any stream capture.  Calls share the scratch: calls whose GPU work
  * overlaps race, so serialise them.  Errors: lbf_last_error(NULL). */
 int lbf_flux_sums_noalloc(const double *u, const double *rho0, const double *rho1,
                           uint32_t n, uint32_t stride, double *out, void *stream);

@@ -7,15 +7,20 @@
 // allocations on their device, or embedded hosts that own every device byte.
 // They pass device pointers for the inputs and for the 9-double output; the
 // per-tile partial sums go to a fixed scratch array compiled into this
-// library (g_flux_scratch, kMaxTiles * 9 doubles = 1,179,648 bytes), which
-// every GPU that loads the library holds until the process exits.
+// library (g_flux_scratch, kMaxTiles * 9 doubles = 1,179,648 bytes).  The
+// array comes into device memory with this library's module: under CUDA's
+// default lazy module loading that happens at the first call on a device
+// (eager loading: when the library's context is set up), and the device
+// then holds it until the process exits.
 //
 // Limits and rules:
 //  - at most kMaxNodes = kTile * kMaxTiles = 16,777,216 nodes per call;
 //    larger n is rejected with LBF_EINVAL before any GPU work;
 //  - the first call on a device looks up the scratch array's device address
-//    (cudaGetSymbolAddress) with that device current; make that first call
-//    before any stream capture;
+//    (cudaGetSymbolAddress) with that device current, which also loads the
+//    module and so needs the 1.2 MB once; make that first call (n = 0 is
+//    enough) while device memory is still free and before any stream
+//    capture;
 //  - all calls share the one scratch array, so calls whose GPU work overlaps
 //    (different streams or threads at the same time) race; serialise them.
 //    Every tile's partial is rewritten by each call before it is read, so

@@ -89,3 +89,21 @@ def test_engine_block_and_density_entry_points_validate():
     assert lib.lbf_block_sums(None, 2, out, 5) == -1
     assert lib.lbf_add_density(None, None) == -1
     assert lib.lbf_initialize_equilibrium(None, None, 4, 0) == -1
+
+
+@pytest.mark.parametrize('args,msg', [
+    (dict(n=(1 << 24) + 1, stride=(1 << 24) + 1), 'exceeds the fixed scratch capacity'),
+    (dict(u=None), 'must be device pointers'),
+    (dict(rho0=None), 'must be device pointers'),
+    (dict(out=None), 'must be device pointers'),
+    (dict(n=100, stride=99), 'stride must be >= n'),
+])
+def test_noalloc_rejects_bad_arguments(args, msg):
+    """lbf_flux_sums_noalloc refuses these before touching the GPU."""
+    import lbflow_b200
+    lib = lbflow_b200.library()
+    a = dict(u=ctypes.c_void_p(16), rho0=ctypes.c_void_p(16), n=10, stride=10, out=ctypes.c_void_p(16))
+    a.update(args)
+    rc = lib.lbf_flux_sums_noalloc(a['u'], a['rho0'], None, a['n'], a['stride'], a['out'], None)
+    assert rc == -1
+    assert msg in lib.lbf_last_error(None).decode()
