@@ -449,12 +449,15 @@ static void scsp_initialize(lbo_sim *s)
 static int scsp_macros(lbo_sim *s)
 {
     const double dens0 = s->p.rho[0];
+    int bad = 0;
+    /* Voxels are independent: the OpenMP split changes no arithmetic. */
+#pragma omp parallel for schedule(static) reduction(|:bad)
     for (size_t i = 0; i < s->N; ++i) {
         if (!is_bulk_type(s->lab[s->geom[i]].type)) continue;
         double r = F(0, 0, i);
         for (int q = 1; q < s->Q; ++q) r += F(0, q, i);
         s->dens[0][i] = r;
-        if (!isfinite(r) || r <= 0.0) return LBO_ERR_DENSITY;
+        if (!isfinite(r) || r <= 0.0) bad = 1;
         for (int d = 0; d < s->D; ++d) {
             double v = 0;
             for (int q = 1; q < s->Q; ++q) {
@@ -464,6 +467,8 @@ static int scsp_macros(lbo_sim *s)
             s->v[d][i] = v / dens0;
         }
     }
+    if (bad) return LBO_ERR_DENSITY;
+#pragma omp parallel for schedule(static)
     for (size_t i = 0; i < s->N; ++i) {
         int label = s->geom[i];
         if (s->lab[label].type != LBO_GV) continue;
@@ -481,6 +486,7 @@ static int scsp_collide(lbo_sim *s)
     const double c1 = 3.0, c2 = 4.5, c3 = 1.5;
     const double omega = 1.0 / s->p.tau[0];
     const double dens0 = s->p.rho[0];
+#pragma omp parallel for schedule(static)
     for (size_t i = 0; i < s->N; ++i) {
         int label = s->geom[i];
         if (!is_fluid_type(s->lab[label].type)) continue;
@@ -519,9 +525,11 @@ static int scsp_collide(lbo_sim *s)
         }
     }
     /* Simulator::validatePopulations (simulator.cpp:327-333). */
+    int bad = 0;
+#pragma omp parallel for schedule(static) reduction(|:bad)
     for (size_t k = 0; k < (size_t)Q * s->N; ++k)
-        if (!isfinite(s->f[k])) return LBO_ERR_NONFINITE;
-    return LBO_OK;
+        if (!isfinite(s->f[k])) bad = 1;
+    return bad ? LBO_ERR_NONFINITE : LBO_OK;
 }
 
 /* SCSP::zouHeBoundary (scsp.cpp:188-275): velocity (VB) and pressure (PB)
@@ -674,32 +682,49 @@ static void color_initialize(lbo_sim *s)
 }
 
 /* ColorFluid::calcMacroVar (colorfluid.cpp:238-290) + bodyForce (:736-750). */
+static int color_macros_voxel(lbo_sim *s, size_t i, double relax0, double relax1)
+{
+    double d0 = F(0, 0, i), d1 = F(1, 0, i);
+    for (int q = 1; q < s->Q; ++q) { d0 += F(0, q, i); d1 += F(1, q, i); }
+    s->dens[0][i] = d0; s->dens[1][i] = d1;
+    double dt = d0 + d1;
+    s->densT[i] = dt;
+    if (!isfinite(d0) || !isfinite(d1) || !isfinite(dt) || dt <= 0.0) return LBO_ERR_DENSITY;
+    if (d0 < -1e-10 * dt || d1 < -1e-10 * dt) return LBO_ERR_COMPONENT;
+    s->densN[i] = (d0 - d1) / dt;
+    s->tau[i] = (1 + s->densN[i]) * relax0 + (1 - s->densN[i]) * relax1;
+    if (!isfinite(s->tau[i]) || s->tau[i] <= 0.5) return LBO_ERR_TAU;
+    for (int d = 0; d < s->D; ++d) {
+        double v = 0;
+        for (int q = 1; q < s->Q; ++q) {
+            if (s->e[q][d] == 1) v += F(0, q, i) + F(1, q, i);
+            else if (s->e[q][d] == -1) v -= F(0, q, i) + F(1, q, i);
+        }
+        v /= dt;
+        s->v[d][i] = v;
+        if (!isfinite(v)) return LBO_ERR_VELOCITY;
+    }
+    return LBO_OK;
+}
+
 static int color_macros(lbo_sim *s)
 {
     const double relax0 = s->p.tau[0] / 2.0, relax1 = s->p.tau[1] / 2.0;
+    int bad = 0;
+    /* Voxels are independent; the first failing voxel in voxel order names
+     * the error, as in the reference's sequential loop. */
+#pragma omp parallel for schedule(static) reduction(|:bad)
     for (size_t i = 0; i < s->N; ++i) {
         if (!is_fluid_type(s->lab[s->geom[i]].type)) continue;
-        double d0 = F(0, 0, i), d1 = F(1, 0, i);
-        for (int q = 1; q < s->Q; ++q) { d0 += F(0, q, i); d1 += F(1, q, i); }
-        s->dens[0][i] = d0; s->dens[1][i] = d1;
-        double dt = d0 + d1;
-        s->densT[i] = dt;
-        if (!isfinite(d0) || !isfinite(d1) || !isfinite(dt) || dt <= 0.0) return LBO_ERR_DENSITY;
-        if (d0 < -1e-10 * dt || d1 < -1e-10 * dt) return LBO_ERR_COMPONENT;
-        s->densN[i] = (d0 - d1) / dt;
-        s->tau[i] = (1 + s->densN[i]) * relax0 + (1 - s->densN[i]) * relax1;
-        if (!isfinite(s->tau[i]) || s->tau[i] <= 0.5) return LBO_ERR_TAU;
-        for (int d = 0; d < s->D; ++d) {
-            double v = 0;
-            for (int q = 1; q < s->Q; ++q) {
-                if (s->e[q][d] == 1) v += F(0, q, i) + F(1, q, i);
-                else if (s->e[q][d] == -1) v -= F(0, q, i) + F(1, q, i);
-            }
-            v /= dt;
-            s->v[d][i] = v;
-            if (!isfinite(v)) return LBO_ERR_VELOCITY;
-        }
+        if (color_macros_voxel(s, i, relax0, relax1) != LBO_OK) bad = 1;
     }
+    if (bad)
+        for (size_t i = 0; i < s->N; ++i) {
+            if (!is_fluid_type(s->lab[s->geom[i]].type)) continue;
+            const int rc = color_macros_voxel(s, i, relax0, relax1);
+            if (rc != LBO_OK) return rc;
+        }
+#pragma omp parallel for schedule(static)
     for (size_t i = 0; i < s->N; ++i) {
         int label = s->geom[i];
         if (s->lab[label].type != LBO_GV) continue;
@@ -774,6 +799,7 @@ static int color_collide(lbo_sim *s)
     double *out1 = malloc(sizeof(double) * (size_t)Q * s->N);
     memcpy(out0, &F(0, 0, 0), sizeof(double) * (size_t)Q * s->N);
     memcpy(out1, &F(1, 0, 0), sizeof(double) * (size_t)Q * s->N);
+#pragma omp parallel for schedule(static)
     for (size_t i = 0; i < s->N; ++i) {
         int label = s->geom[i];
         if (!is_fluid_type(s->lab[label].type)) continue;
@@ -858,9 +884,11 @@ static int color_collide(lbo_sim *s)
     memcpy(&F(0, 0, 0), out0, sizeof(double) * (size_t)Q * s->N);
     memcpy(&F(1, 0, 0), out1, sizeof(double) * (size_t)Q * s->N);
     free(out0); free(out1);
+    int bad = 0;
+#pragma omp parallel for schedule(static) reduction(|:bad)
     for (size_t k = 0; k < 2 * (size_t)Q * s->N; ++k)
-        if (!isfinite(s->f[k])) return LBO_ERR_NONFINITE;
-    return LBO_OK;
+        if (!isfinite(s->f[k])) bad = 1;
+    return bad ? LBO_ERR_NONFINITE : LBO_OK;
 }
 
 /* ---- common step pieces ----------------------------------------------------- */
@@ -874,13 +902,14 @@ static void stream_bounce(lbo_sim *s)
     memcpy(s->fold, s->f, total * sizeof(double));
     for (int ph = 0; ph < s->phases; ++ph)
         for (int q = 1; q < s->Q; ++q) {
-            const int opq = s->op[q];
+            /* adj(., q) is a bijection of the voxels: each target is written once. */
+#pragma omp parallel for schedule(static)
             for (size_t i = 0; i < s->N; ++i) F(ph, q, adj(s, i, q)) = FO(ph, q, i);
-            (void)opq;
         }
     for (int ph = 0; ph < s->phases; ++ph)
         for (int q = 1; q < s->Q; ++q) {
             const int opq = s->op[q];
+#pragma omp parallel for schedule(static)
             for (size_t i = 0; i < s->N; ++i)
                 if (s->link[i] & (1u << (q - 1))) F(ph, opq, i) = FO(ph, q, i);
         }
