@@ -38,7 +38,6 @@ METRIC = 'D3Q19 MRT fluid MLUPS (256^3 porous cube, porosity 0.22)'
 ALG_BYTES = {'fp64': 2 * 19 * 8 + 4, 'fp32': 2 * 19 * 4 + 4, 'fp16': 2 * 19 * 2 + 4, 'bf16': 2 * 19 * 2 + 4,
              'bfp16': 2 * 19 * 2 + 2 + 4}
 ELEM = {'fp64': 8, 'fp32': 4, 'fp16': 2, 'bf16': 2, 'bfp16': 2}
-REF_SAMPLE = dict(n=64, sigma=3.0, porosity=0.22, seed=0)
 
 
 def measured_peaks():
@@ -125,12 +124,18 @@ def make_geometry(n, sigma, porosity, seed):
 LABELS = {75: ('GV', 1e-5, 1, 0), 255: ('SD', 90.0, 0, 0)}
 
 
-def reference_run(workdir, geometry, steps, collision='MRT'):
-    """Run the reference LBFlow binary once; return (fluid_nodes, steps, numerical seconds)."""
+def reference_run(workdir, geometry, steps, collision='MRT', grid_file=None):
+    """Run the reference LBFlow binary once; return (fluid_nodes, steps, numerical seconds).
+    Outputs go to workdir; field writes only at t = 0 (the reference always
+    writes the initial fields), no checkpoint."""
     exe = ROOT / 'oracle' / '_ref' / 'LBFlow'
     nz, ny, nx = geometry.shape
     workdir.mkdir(parents=True, exist_ok=True)
-    geometry.tofile(workdir / 'geometry.raw')
+    if grid_file is None:
+        geometry.tofile(workdir / 'geometry.raw')
+    else:
+        (workdir / 'geometry.raw').symlink_to(grid_file)
+    quiet = steps * 10
     prm = f'''gridFile "geometry.raw";
 dimension {nz} {ny} {nx};
 directions 19;
@@ -138,9 +143,9 @@ fileType "uint8";
 latticeLen 1;
 startTime 0;
 endTime {steps};
-writeInterval {steps};
-reportInterval {steps};
-restartInterval {steps * 10};
+writeInterval {quiet};
+reportInterval {quiet};
+restartInterval {quiet};
 stopError 1e-6;
 outPath "field";
 logPath ".";
@@ -166,36 +171,102 @@ interfaceThickness 0.7;
     return t['fluid_nodes'], t['completed_steps'], t['numerical_seconds_max']
 
 
-def reference_sample(steps, procs):
-    """The reference solver on a bounded sample: `procs` concurrent single-rank runs
-    of the 64^3 crop of the same recipe; aggregate fluid MLUPS."""
+# Peak resident memory of one reference process on the 256^3 cube (measured:
+# 13.6 GB; the reference builds per-voxel adjacency arrays), with headroom.
+REF_BYTES_256 = 16e9
+
+
+def host_memory_available():
+    """Bytes this process may still use: MemAvailable, capped by a cgroup limit."""
+    avail = None
+    try:
+        for line in open('/proc/meminfo'):
+            if line.startswith('MemAvailable:'):
+                avail = int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    for path in ('/sys/fs/cgroup/memory.max', '/sys/fs/cgroup/memory/memory.limit_in_bytes'):
+        try:
+            lim = open(path).read().strip()
+            used_p = path.replace('memory.max', 'memory.current').replace('limit_in_bytes', 'usage_in_bytes')
+            if lim != 'max':
+                used = int(open(used_p).read().strip())
+                room = int(lim) - used
+                avail = room if avail is None else min(avail, room)
+            break
+        except (OSError, ValueError):
+            continue
+    return avail
+
+
+def host_cores():
+    """Logical CPUs this process may run on, and physical cores (lscpu)."""
+    try:
+        logical = len(os.sched_getaffinity(0))
+    except AttributeError:
+        logical = os.cpu_count() or 1
+    physical = None
+    try:
+        out = subprocess.run(['lscpu', '-p=CORE,SOCKET'], capture_output=True, text=True, timeout=10).stdout
+        physical = len({l for l in out.splitlines() if l and not l.startswith('#')})
+    except (OSError, subprocess.SubprocessError):
+        pass
+    return logical, physical
+
+
+def reference_sample(steps, procs, size=256):
+    """The reference solver on the benchmark's own workload: `procs`
+    concurrent single-rank runs of the size^3 cube (sigma 3, porosity 0.22,
+    seed 0 -- the geometry of the GPU arm), each `steps` steps after its
+    initialization; aggregate fluid MLUPS = sum(fluid nodes x steps) / the
+    slowest run's numerical seconds (scripts/performance.py:80-85)."""
     exe = ROOT / 'oracle' / '_ref' / 'LBFlow'
     if not exe.exists():
         return None, 'reference binary oracle/_ref/LBFlow is not built'
-    g = make_geometry(REF_SAMPLE['n'], REF_SAMPLE['sigma'], REF_SAMPLE['porosity'], REF_SAMPLE['seed'])
+    g = make_geometry(size, 3.0, 0.22, 0)
+    logical, physical = host_cores()
     with tempfile.TemporaryDirectory() as d:
+        shared = Path(d) / 'geometry.raw'
+        g.tofile(shared)
         import concurrent.futures as cf
         with cf.ThreadPoolExecutor(procs) as ex:
-            res = list(ex.map(lambda k: reference_run(Path(d) / f'r{k}', g, steps), range(procs)))
+            res = list(ex.map(lambda k: reference_run(Path(d) / f'r{k}', g, steps, grid_file=shared), range(procs)))
     nodes = sum(r[0] * r[1] for r in res)
     secs = max(r[2] for r in res)
     return dict(value=nodes / secs / 1e6, unit='MLUPS', cores=procs, kind='reference',
-                sample=f'{procs} x reference LBFlow (1 rank each) on the 64^3 crop of the same recipe '
-                       f'(sigma 3, porosity 0.22, seed 0, {res[0][0]} fluid nodes), MRT FP64, {steps} steps'), None
+                host_logical_cpus=logical, host_physical_cores=physical,
+                sample=f'{procs} x reference LBFlow (1 rank each, no MPI on the host) on the {size}^3 cube of '
+                       f'the benchmark (sigma 3, porosity 0.22, seed 0, {res[0][0]} fluid nodes), MRT FP64, '
+                       f'{steps} steps each after initialization'), None
+
+
+def reference_procs(limit=None):
+    """Concurrent reference processes: one per logical CPU, as many as host
+    memory holds at 16 GB each."""
+    logical, _ = host_cores()
+    avail = host_memory_available()
+    by_mem = int(avail // REF_BYTES_256) if avail else 1
+    n = max(1, min(logical, by_mem))
+    return min(n, limit) if limit else n
 
 
 def run_reference_arm(args):
     rank = int(os.environ.get('RANK', '0'))
     if rank != 0:
         return 0
-    procs = max(1, min(os.cpu_count() or 1, 16))
-    steps = max(1, args.steps + args.warmup)
+    procs = reference_procs(limit=args.ref_procs)
+    # A bounded sample of the workload: each process runs a few steps of the
+    # full cube (about 6 s per step per core), so the arm ends in a few
+    # minutes whatever --steps is.
+    steps = max(1, min(args.steps + args.warmup, args.ref_steps))
     base, why = reference_sample(steps, procs)
-    cfg = dict(workload='D3Q19 MRT FP64 porous cube, reference solver on a 64^3 sample',
-               porosity=0.22, sigma=3, tau=1.0, g_x=1e-5)
+    cfg = dict(workload='D3Q19 MRT single-phase porous cube 256^3, fp64 populations (reference solver)',
+               nx=256, ny=256, nz=256, porosity=0.22, sigma=3, tau=1.0, g_x=1e-5, seed=0,
+               parallelism=f'{procs} independent single-rank processes')
     if base is None:
         print(json.dumps({'impl': 'reference', 'unavailable': why}))
         return 0
+    cfg['fluid_nodes'] = int(base['sample'].split(' fluid nodes')[0].rsplit(' ', 1)[-1])
     line = dict(impl='reference', metric=METRIC, value=base['value'], unit='MLUPS', n_gpus=args.gpus,
                 steps=args.steps, warmup=args.warmup, ms_per_step=None, higher_is_better=True,
                 scaling='weak', vs_baseline=None, dtype='f64', data='synthetic', config=cfg,
@@ -246,6 +317,8 @@ def main():
     ap.add_argument('--warm-weights', default=str(Path(__file__).resolve().parent / 'lbflow_b200' / 'weights' /
                                                   'warmstart.pt'), help='ttp: trained warm-start operator')
     ap.add_argument('--check', type=int, default=8, help='batch: geometries re-solved alone in FP64')
+    ap.add_argument('--ref-steps', type=int, default=3, help='reference arm: steps per reference process')
+    ap.add_argument('--ref-procs', type=int, default=None, help='reference arm: cap on concurrent processes')
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -325,7 +398,7 @@ def main():
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        base, _ = reference_sample(steps=100, procs=1)
+        base, _ = reference_sample(steps=2, procs=1)
 
     if rank == 0:
         clk = clocks.summary()
@@ -728,26 +801,37 @@ def operator_run(args):
     return 0
 
 def end_to_end(geometry, args, device):
-    """Same metric through the C ABI with host buffers: geometry upload and
-    classification, initialization, K steps each followed by the read-back of
-    the step's flux and mass sums, then the final density/velocity download."""
-    from lbflow_b200 import Engine
+    """Same metric through the C ABI with host buffers: the uint8 geometry
+    from the host (classified on the device), initialization, K steps each
+    followed by the read-back of the step's flux and mass sums (the numbers
+    K is computed from), then the final density and velocity fields in the
+    VTI layout into page-locked host memory.  The page-locked output buffer
+    is allocated before the timed region, as a caller reusing it would."""
+    from lbflow_b200 import Engine, HostBuffer
     import torch
+    fields = HostBuffer(4 * geometry.size)
+    geom = np.ascontiguousarray(geometry)
     torch.cuda.synchronize()
     t = time.perf_counter()
-    eng = Engine(geometry, LABELS, model='scsp', collision=args.collision, tau=(1.0,), rho=(1.0,),
+    eng = Engine(geom, LABELS, model='scsp', collision=args.collision, tau=(1.0,), rho=(1.0,),
                  storage=args.storage, device=device)
     eng.initialize()
+    sums = None
     for _ in range(args.steps):
         eng.step(1, macros=True)
-        eng.flux_sums()
-    r0, _, u = eng.macros()
+        sums = eng.flux_sums()
+    eng.fields_dense_async(fields.ptr.value, fields.count)
+    eng.synchronize()
     eng.check()
     dt = time.perf_counter() - t
     nf = eng.fluid_nodes
     eng.close()
+    ok = bool(np.isfinite(fields.array[::4097]).all()) and sums is not None and np.isfinite(sums).all()
+    fields.close()
+    if not ok:
+        raise RuntimeError('end-to-end run produced non-finite output')
     h2d = geometry.nbytes + 256 * 24
-    d2h = 9 * 8 * args.steps + r0.nbytes + u.nbytes
+    d2h = 9 * 8 * args.steps + 4 * 8 * geometry.size
     return dict(value=nf * args.steps / dt / 1e6, unit='MLUPS',
                 h2d_bytes_per_step=h2d / args.steps, d2h_bytes_per_step=d2h / args.steps,
                 seconds=dt)

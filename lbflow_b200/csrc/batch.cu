@@ -8,7 +8,11 @@
 // one geometry (all-solid regions produce no nodes and so no tiles); a grid of
 // resident blocks walks the tile list of the still-active geometries every
 // step, reading each tile's geometry size and collision rates.  Steps are
-// replayed from a captured CUDA graph.  Per-geometry reductions write one
+// replayed from a captured CUDA graph.  FP16 storage rounds stochastically
+// with the single engine's per-step seeds: the step count lives in device
+// memory (a pair of words indexed by the buffer parity: a step reads one and
+// its first thread writes the next count into the other), so graph replays
+// see a new seed every step without any host involvement.  Per-geometry reductions write one
 // partial per tile and then sum each geometry's tiles in order
 // (deterministic), so every geometry can be tested for convergence and
 // retired on its own.  lbf_batch_autotune picks the tile size and grid shape
@@ -46,8 +50,19 @@ __global__ void __launch_bounds__(256)
 batch_step(const BatchGeom* __restrict__ geoms, const Tile* __restrict__ tiles, uint32_t ntiles,
            const uint2* __restrict__ occ, const uint32_t* __restrict__ coord, uint32_t nfp,
            const Force F, const double rho0, const typename S::T* __restrict__ fin,
-           typename S::T* __restrict__ fout, Macros mo, const int out, uint32_t* __restrict__ err)
+           typename S::T* __restrict__ fout, Macros mo, const int out, uint32_t* __restrict__ err,
+           uint32_t* __restrict__ step_count, const int parity)
 {
+    // Stochastic rounding seed of this step (16-bit float storage, pull
+    // steps): count k = 1, 2, ... of pull steps, as the single engine seeds
+    // them.  This launch reads step_count[parity] and publishes k into
+    // step_count[parity ^ 1] for the next launch, never the word it reads.
+    uint32_t seed = 0;
+    if (S::dither && PULL && step_count) {
+        const uint32_t k = step_count[parity] + 1u;
+        seed = (k * 2654435761u) | 1u;
+        if (blockIdx.x == 0 && threadIdx.x == 0) step_count[parity ^ 1] = k;
+    }
     for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const Tile tl = tiles[t];
         const BatchGeom G = geoms[tl.geom];
@@ -62,6 +77,8 @@ batch_step(const BatchGeom* __restrict__ geoms, const Tile* __restrict__ tiles, 
         P.inv_rho0 = 1.0 / rho0;
         P.rate.sp = G.sp;
         P.rate.sm = G.sm;
+        P.seed = seed;
+        P.node0 = G.node_base;
         for (uint32_t k = threadIdx.x; k < tl.count; k += blockDim.x)
             scsp_update<L, S, PULL>(g, F, P, fin, fout, tl.first + k, mo, out, err, nullptr, nullptr);
     }
@@ -145,6 +162,7 @@ struct lbf_batch {
     uint32_t* d_tile_count = nullptr;
     double* d_partial = nullptr;
     double* d_out = nullptr;
+    uint32_t* d_step = nullptr;       // pull-step count, two words by buffer parity (FP16 rounding seeds)
     uint32_t ntiles_all = 0, ntiles_active = 0;
     std::vector<Tile> tiles_all;
     std::vector<uint32_t> tile_first, tile_count;
@@ -192,11 +210,11 @@ void launch_batch(lbf_batch* b, bool pull, int out, const Tile* tiles, uint32_t 
     if (pull)
         batch_step<D3Q19, S, true><<<grid, b->threads, 0, b->stream>>>(
             b->d_geoms, tiles, ntiles, b->d_occ, b->d_coord, b->nfp, b->force, b->rho0, fin, fout,
-            batch_macros(b), out, b->err);
+            batch_macros(b), out, b->err, b->d_step, b->cur);
     else
         batch_step<D3Q19, S, false><<<grid, b->threads, 0, b->stream>>>(
             b->d_geoms, tiles, ntiles, b->d_occ, b->d_coord, b->nfp, b->force, b->rho0, fin, fout,
-            batch_macros(b), out, b->err);
+            batch_macros(b), out, b->err, b->d_step, b->cur);
 }
 
 void batch_launch(lbf_batch* b, bool pull, int out, bool all_tiles = false)
@@ -419,6 +437,8 @@ int lbf_batch_create(const lbf_batch_geometry* geoms, uint32_t count, const lbf_
     BALLOC(b->uadj, (size_t)3 * b->nfp * sizeof(double));
     BALLOC(b->err, sizeof(uint32_t));
     BALLOC(b->d_out, (size_t)count * kReduceMaxK * sizeof(double));
+    BALLOC(b->d_step, 2 * sizeof(uint32_t));
+    BCUDA(cudaMemsetAsync(b->d_step, 0, 2 * sizeof(uint32_t), b->stream));
     BCUDA(cudaMemsetAsync(b->rho, 0, (size_t)b->nfp * sizeof(double), b->stream));
     BCUDA(cudaMemsetAsync(b->u, 0, (size_t)3 * b->nfp * sizeof(double), b->stream));
     BCUDA(cudaMemsetAsync(b->uprev, 0, (size_t)3 * b->nfp * sizeof(double), b->stream));
@@ -454,7 +474,7 @@ void lbf_batch_destroy(lbf_batch* b)
     drop_graph(b);
     void* ptrs[] = {b->d_geoms, b->d_occ, b->d_coord, b->d_label, b->d_label_force, b->f[0], b->f[1],
                     b->rho, b->u, b->uprev, b->uadj, b->err, b->d_tiles_all, b->d_tiles_active,
-                    b->d_tile_first, b->d_tile_count, b->d_partial, b->d_out};
+                    b->d_tile_first, b->d_tile_count, b->d_partial, b->d_out, b->d_step};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
@@ -554,8 +574,10 @@ int lbf_batch_autotune(lbf_batch* b, uint32_t steps, double out[4])
     // so that tuning leaves the simulation where it was.
     const size_t fbytes = (size_t)19 * b->nfp * b->elem;
     void* snap = nullptr;
-    BCK(b, cudaMalloc(&snap, fbytes));
+    BCK(b, cudaMalloc(&snap, fbytes + 2 * sizeof(uint32_t)));
     BCK(b, cudaMemcpyAsync(snap, b->f[b->cur], fbytes, cudaMemcpyDeviceToDevice, b->stream));
+    BCK(b, cudaMemcpyAsync((char*)snap + fbytes, b->d_step, 2 * sizeof(uint32_t), cudaMemcpyDeviceToDevice, b->stream));
+    const int cur0 = b->cur;
     cudaEvent_t e0, e1;
     BCK(b, cudaEventCreate(&e0));
     BCK(b, cudaEventCreate(&e1));
@@ -579,8 +601,10 @@ int lbf_batch_autotune(lbf_batch* b, uint32_t steps, double out[4])
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     BCK(b, cudaMemcpyAsync(b->f[b->cur], snap, fbytes, cudaMemcpyDeviceToDevice, b->stream));
+    BCK(b, cudaMemcpyAsync(b->d_step, (char*)snap + fbytes, 2 * sizeof(uint32_t), cudaMemcpyDeviceToDevice, b->stream));
     BCK(b, cudaStreamSynchronize(b->stream));
     cudaFree(snap);
+    if (b->cur != cur0) return bfail(b, LBF_ESTATE, "autotune: buffer parity changed");
     b->threads = bt;
     b->tile_nodes = btile;
     b->grid = bgrid;

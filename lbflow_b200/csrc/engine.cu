@@ -4,6 +4,9 @@
 #include "internal.h"
 #include "reduce.cuh"
 
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -425,6 +428,130 @@ unsigned dense_blocks(size_t N)
 }
 }  // namespace
 
+namespace {
+// ---- geometry classification on the device ---------------------------------
+// One warp per 32-voxel occupancy word of an x-row (words in z, y, x-word
+// order): lane b reads voxel x = 32 w + b, the warp's ballot of "carries
+// populations" is the word's fluid bits.  Also records which labels occur
+// (an 8-word bitmap) and each word's fluid count for the prefix scan.
+__global__ void classify_words(const uint8_t* __restrict__ geom, const uint8_t* __restrict__ fluid_label, int nx,
+                               int W, size_t words, uint2* __restrict__ occ, unsigned long long* __restrict__ counts,
+                               uint32_t* __restrict__ used)
+{
+    __shared__ uint32_t s_used[8];
+    if (threadIdx.x < 8) s_used[threadIdx.x] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const size_t warps = ((size_t)gridDim.x * blockDim.x) >> 5;
+    for (size_t wd = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; wd < words; wd += warps) {
+        const size_t r = wd / (size_t)W;
+        const int x = (int)(wd - r * W) * 32 + lane;
+        bool fl = false;
+        uint32_t word = 8, bit = 0;
+        if (x < nx) {
+            const uint8_t l = geom[r * (size_t)nx + x];
+            fl = fluid_label[l] != 0;
+            word = l >> 5;
+            bit = 1u << (l & 31);
+        }
+        const uint32_t bits = __ballot_sync(0xffffffffu, fl);
+#pragma unroll
+        for (uint32_t k = 0; k < 8; ++k) {
+            const uint32_t m = __reduce_or_sync(0xffffffffu, word == k ? bit : 0u);
+            if (lane == 0 && m) atomicOr(&s_used[k], m);
+        }
+        if (lane == 0) {
+            occ[wd].x = bits;
+            counts[wd] = (unsigned long long)__popc(bits);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 8 && s_used[threadIdx.x]) atomicOr(&used[threadIdx.x], s_used[threadIdx.x]);
+}
+
+// Prefix counts into the words; total[0] = number of fluid voxels.
+__global__ void finish_words(const unsigned long long* __restrict__ counts,
+                             const unsigned long long* __restrict__ prefix, size_t words, uint2* __restrict__ occ,
+                             unsigned long long* __restrict__ total)
+{
+    for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < words; w += (size_t)gridDim.x * blockDim.x) {
+        occ[w].y = (uint32_t)prefix[w];
+        if (w + 1 == words) total[0] = prefix[w] + counts[w];
+    }
+}
+
+// Node records in voxel order: packed coordinates, and where needed the
+// node's label (per-label forces) and phase (two-phase initialisation).
+__global__ void fill_nodes(const uint8_t* __restrict__ geom, const uint2* __restrict__ occ, int nx, int ny, int W,
+                           size_t words, const uint8_t* __restrict__ phase_of, uint32_t* __restrict__ coord,
+                           uint8_t* __restrict__ nlabel, uint8_t* __restrict__ nphase)
+{
+    const int lane = threadIdx.x & 31;
+    const size_t warps = ((size_t)gridDim.x * blockDim.x) >> 5;
+    for (size_t wd = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; wd < words; wd += warps) {
+        const uint2 e = occ[wd];
+        if (!((e.x >> lane) & 1u)) continue;
+        const size_t r = wd / (size_t)W;
+        const uint32_t x = (uint32_t)(wd - r * W) * 32 + lane;
+        const uint32_t y = (uint32_t)(r % (size_t)ny), z = (uint32_t)(r / (size_t)ny);
+        const uint32_t k = e.y + __popc(e.x & ((1u << lane) - 1u));
+        coord[k] = x | (y << 11) | (z << 22);
+        const uint8_t l = geom[r * (size_t)nx + x];
+        if (nlabel) nlabel[k] = l;
+        if (nphase) nphase[k] = phase_of[l];
+    }
+}
+
+// Voxel index of every node from the device coordinates (host copy, built on
+// the first call that needs it: dense host transfers and set-up lists).
+int ensure_vox(lbf_engine* e)
+{
+    if (e->vox.size() == e->nf) return LBF_OK;
+    std::vector<uint32_t> c(e->nf);
+    if (e->nf) {
+        LBF_CK(e, cudaMemcpyAsync(c.data(), e->coord, (size_t)e->nf * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                  e->stream));
+        LBF_CK(e, cudaStreamSynchronize(e->stream));
+    }
+    e->vox.resize(e->nf);
+    for (uint32_t k = 0; k < e->nf; ++k) {
+        const uint32_t x = c[k] & 2047u, y = (c[k] >> 11) & 2047u, z = c[k] >> 22;
+        e->vox[k] = (uint32_t)(((size_t)z * e->ny + y) * e->nx + x);
+    }
+    return LBF_OK;
+}
+
+// Label checks (ValidateSimulation subset, fileprm.cpp:274-294) over the
+// labels that occur, and the fluid/solid type sets of buildIb
+// (simulator.cpp:399-415).
+int validate_labels(const lbf_config& c, const lbf_label* labels, const bool (&used)[256], int Q, int D,
+                    int phases, std::string& msg)
+{
+    for (int l = 0; l < 256; ++l) {
+        if (!used[l]) continue;
+        const lbf_label& L = labels[l];
+        msg.clear();
+        if (L.type == 0) msg = "geometry label " + std::to_string(l) + " is not defined";
+        else if (!is_fluid(L.type) && !is_solid(L.type))
+            msg = "label " + std::to_string(l) + ": only VD, GV, PB, VB, HF, BB and SD labels are supported";
+        else if (L.type == LBF_HF && c.model != LBF_MODEL_COLOR)
+            msg = "label " + std::to_string(l) + ": half-permeable films (HF) need the color model";
+        else if ((L.type == LBF_PB || L.type == LBF_VB) && !std::isfinite(L.value)) msg = "Non-finite boundary value.";
+        else if ((L.type == LBF_PB || L.type == LBF_VB) && (L.dir <= 0 || L.dir >= Q))
+            msg = "Boundary direction must be a non-rest lattice direction.";
+        else if (L.type == LBF_PB && L.value <= 0.0) msg = "Pressure-boundary density must be positive.";
+        else if ((L.type == LBF_PB || L.type == LBF_VB) && L.dir > 2 * D)
+            msg = "Pressure and velocity boundaries require an axial direction.";
+        else if (is_fluid(L.type) && (L.phase < 0 || L.phase >= phases))
+            msg = "Boundary phase is outside the configured fluid model.";
+        else if (L.type == LBF_GV && (L.dir <= 0 || L.dir >= Q || !std::isfinite(L.value)))
+            msg = "Invalid body-force direction or magnitude.";
+        if (!msg.empty()) return LBF_EINVAL;
+    }
+    return LBF_OK;
+}
+}  // namespace
+
 extern "C" {
 
 int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t* geometry, lbf_engine** out)
@@ -464,82 +591,99 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
     const bool blocked = c.storage == LBF_STORE_BFP16;
     auto bail = [&](int code, const std::string& m) { lbf_destroy(e); return fail(nullptr, code, m); };
 
-    // Label checks (ValidateSimulation subset, fileprm.cpp:274-294) and the
-    // fluid/solid type sets of buildIb (simulator.cpp:399-415).
+    // Which labels occur, the occupancy words and the fluid count come from
+    // the device (classify_words); without a usable device the labels are
+    // still checked on the host so that a bad geometry is reported as such.
     bool used[256] = {};
-    for (size_t v = 0; v < e->N; ++v) used[geometry[v]] = true;
-    for (int l = 0; l < 256; ++l) {
-        if (!used[l]) continue;
-        const lbf_label& L = labels[l];
-        if (L.type == 0) return bail(LBF_EINVAL, "geometry label " + std::to_string(l) + " is not defined");
-        if (!is_fluid(L.type) && !is_solid(L.type))
-            return bail(LBF_EINVAL, "label " + std::to_string(l) + ": only VD, GV, PB, VB, HF, BB and SD labels are supported");
-        if (L.type == LBF_HF && c.model != LBF_MODEL_COLOR)
-            return bail(LBF_EINVAL, "label " + std::to_string(l) + ": half-permeable films (HF) need the color model");
-        if ((L.type == LBF_PB || L.type == LBF_VB) && !std::isfinite(L.value))
-            return bail(LBF_EINVAL, "Non-finite boundary value.");
-        if ((L.type == LBF_PB || L.type == LBF_VB) && (L.dir <= 0 || L.dir >= e->Q))
-            return bail(LBF_EINVAL, "Boundary direction must be a non-rest lattice direction.");
-        if (L.type == LBF_PB && L.value <= 0.0)
-            return bail(LBF_EINVAL, "Pressure-boundary density must be positive.");
-        if ((L.type == LBF_PB || L.type == LBF_VB) && L.dir > 2 * e->D)
-            return bail(LBF_EINVAL, "Pressure and velocity boundaries require an axial direction.");
-        if (is_fluid(L.type) && (L.phase < 0 || L.phase >= phases))
-            return bail(LBF_EINVAL, "Boundary phase is outside the configured fluid model.");
-        if (L.type == LBF_GV && (L.dir <= 0 || L.dir >= e->Q || !std::isfinite(L.value)))
-            return bail(LBF_EINVAL, "Invalid body-force direction or magnitude.");
-    }
-
-    // Occupancy words with prefix counts; fluid nodes in voxel order.
     const size_t rows = (size_t)e->nz * e->ny;
-    std::vector<uint2> occ(rows * e->W);
+    const size_t words = rows * (size_t)e->W;
+    int rc = setdev(e);
+    if (rc) {
+        for (size_t v = 0; v < e->N; ++v) used[geometry[v]] = true;
+        std::string m;
+        if (validate_labels(c, labels, used, e->Q, e->D, phases, m) != LBF_OK) return bail(LBF_EINVAL, m);
+        m = e->last_error;
+        lbf_destroy(e);
+        return fail(nullptr, rc, m);
+    }
+#define LBF_ALLOC(p, n)                                                  \
+    do {                                                                 \
+        int r_ = dalloc(e, &(p), (n));                                   \
+        if (r_) { std::string m_ = e->last_error; lbf_destroy(e); return fail(nullptr, r_, m_); } \
+    } while (0)
+#define LBF_CUDA(call)                                                   \
+    do {                                                                 \
+        cudaError_t r_ = (call);                                         \
+        if (r_ != cudaSuccess) { lbf_destroy(e); return fail(nullptr, LBF_ECUDA, std::string(#call) + ": " + cudaGetErrorString(r_)); } \
+    } while (0)
+    LBF_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+    LBF_CUDA(cudaMallocHost(&e->h_red, kReduceMaxK * sizeof(double)));
+    // Set-up scratch, freed before returning: the geometry, per-label tables
+    // (fluid flag, phase), word counts and their prefix, the label bitmap and
+    // the fluid total.
+    uint8_t* d_geom = nullptr;
+    uint8_t* d_ltab = nullptr;
+    unsigned long long* d_cnt = nullptr;
+    void* d_scan_tmp = nullptr;
+    size_t scan_bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                  (int64_t)words);
+    struct Scratch {
+        void* p[4] = {nullptr, nullptr, nullptr, nullptr};
+        ~Scratch() { for (void* q : p) if (q) cudaFree(q); }
+    } scratch;
+    auto salloc = [&](void** p, size_t bytes, int slot) -> cudaError_t {
+        const cudaError_t r = cudaMalloc(p, bytes ? bytes : 1);
+        if (r == cudaSuccess) scratch.p[slot] = *p;
+        return r;
+    };
+    LBF_CUDA(salloc((void**)&d_geom, e->N, 0));
+    LBF_CUDA(salloc((void**)&d_ltab, 512, 1));
+    LBF_CUDA(salloc((void**)&d_cnt, (2 * words + 2) * sizeof(unsigned long long) + 8 * sizeof(uint32_t), 2));
+    LBF_CUDA(salloc(&d_scan_tmp, scan_bytes, 3));
+    unsigned long long* d_prefix = d_cnt + words;
+    unsigned long long* d_total = d_prefix + words;
+    uint32_t* d_used = reinterpret_cast<uint32_t*>(d_total + 2);
+    uint8_t ltab[512];
+    for (int l = 0; l < 256; ++l) {
+        ltab[l] = is_fluid(labels[l].type) ? 1 : 0;
+        ltab[256 + l] = (uint8_t)(is_fluid(labels[l].type) && labels[l].phase >= 0 && labels[l].phase < 2
+                                  ? labels[l].phase : 0);
+    }
+    LBF_ALLOC(e->occ, words);
+    LBF_CUDA(cudaMemcpyAsync(d_geom, geometry, e->N, cudaMemcpyHostToDevice, e->stream));
+    LBF_CUDA(cudaMemcpyAsync(d_ltab, ltab, sizeof ltab, cudaMemcpyHostToDevice, e->stream));
+    LBF_CUDA(cudaMemsetAsync(d_total, 0, 2 * sizeof(unsigned long long) + 8 * sizeof(uint32_t), e->stream));
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, (int)c.device);
+    const unsigned cls_blocks = (unsigned)std::min<size_t>((words + 7) / 8, (size_t)sms * 16);
+    classify_words<<<cls_blocks, 256, 0, e->stream>>>(d_geom, d_ltab, e->nx, e->W, words, e->occ, d_cnt, d_used);
+    LBF_CUDA(cudaGetLastError());
+    LBF_CUDA(cub::DeviceScan::ExclusiveSum(d_scan_tmp, scan_bytes, d_cnt, d_prefix, (int64_t)words, e->stream));
+    finish_words<<<(unsigned)std::min<size_t>((words + 255) / 256, (size_t)sms * 16), 256, 0, e->stream>>>(
+        d_cnt, d_prefix, words, e->occ, d_total);
+    LBF_CUDA(cudaGetLastError());
+    static_assert(kReduceMaxK * sizeof(double) >= 8 + 8 * sizeof(uint32_t), "pinned staging too small");
+    LBF_CUDA(cudaMemcpyAsync(e->h_red, d_total, 8 + 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream));
+    // d_total + 1 is unused padding; the bitmap follows it.
+    LBF_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(e->h_red) + 8, d_used, 8 * sizeof(uint32_t),
+                             cudaMemcpyDeviceToHost, e->stream));
+    LBF_CUDA(cudaStreamSynchronize(e->stream));
     uint64_t count = 0;
-    for (size_t r = 0; r < rows; ++r)
-        for (int w = 0; w < e->W; ++w) {
-            uint32_t bits = 0;
-            for (int b = 0; b < 32; ++b) {
-                const int x = w * 32 + b;
-                if (x >= e->nx) break;
-                if (is_fluid(labels[geometry[r * e->nx + x]].type)) bits |= 1u << b;
-            }
-            occ[r * e->W + w] = make_uint2(bits, (uint32_t)count);
-            count += (uint64_t)__builtin_popcount(bits);
-        }
+    uint32_t used_bits[8];
+    std::memcpy(&count, e->h_red, 8);
+    std::memcpy(used_bits, reinterpret_cast<char*>(e->h_red) + 8, sizeof used_bits);
+    for (int l = 0; l < 256; ++l) used[l] = (used_bits[l >> 5] >> (l & 31)) & 1u;
+    {
+        std::string m;
+        if (validate_labels(c, labels, used, e->Q, e->D, phases, m) != LBF_OK) return bail(LBF_EINVAL, m);
+    }
     // Element offsets inside a population buffer are 32-bit in the kernels.
     if ((count + 64) * (uint64_t)phases * (uint64_t)e->Q >= 0xffffffffull)
         return bail(LBF_EINVAL, "too many fluid nodes for one engine (phases * Q * nodes must stay below 2^32)");
     e->nf = (uint32_t)count;
     e->nfp = (uint32_t)((count + 63) / 64 * 64);
     if (e->nfp == 0) e->nfp = 64;
-    e->vox.resize(e->nf);
-    std::vector<uint32_t> coord(e->nf);
-    std::vector<uint8_t> nlabel(e->nf), nphase(e->nf);
-    {
-        uint32_t k = 0;
-        for (size_t v = 0; v < e->N; ++v) {
-            const uint8_t l = geometry[v];
-            if (!is_fluid(labels[l].type)) continue;
-            const uint32_t x = (uint32_t)(v % e->nx), y = (uint32_t)((v / e->nx) % e->ny),
-                           z = (uint32_t)(v / ((size_t)e->nx * e->ny));
-            e->vox[k] = (uint32_t)v;
-            coord[k] = x | (y << 11) | (z << 22);
-            nlabel[k] = l;
-            nphase[k] = (uint8_t)labels[l].phase;
-            ++k;
-        }
-    }
-
-    // Zou-He boundary nodes in compact order (SCSP::zouHeBoundary, scsp.cpp:188-275).
-    std::vector<uint32_t> zh_node, zh_code;
-    std::vector<double> zh_value;
-    for (uint32_t k = 0; k < e->nf; ++k) {
-        const lbf_label& L = labels[nlabel[k]];
-        if (L.type != LBF_PB && L.type != LBF_VB) continue;
-        zh_node.push_back(k);
-        zh_code.push_back(((uint32_t)L.phase << 16) | ((L.type == LBF_VB ? kZouHeVB : kZouHePB) << 8) |
-                          (uint32_t)L.dir);
-        zh_value.push_back(L.value);
-    }
 
     // Body force per label, x/y/z (Simulator::forceForIndex, simulator.cpp:218-228:
     // Qp[dir] * value, Qp = e / |e|).
@@ -563,20 +707,9 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
         if (first) { for (int a = 0; a < 3; ++a) F0[a] = lforce[3 * l + a]; first = false; }
         else for (int a = 0; a < 3; ++a) if (lforce[3 * l + a] != F0[a]) uniform = false;
     }
+    bool boundaries = false;
+    for (int l = 0; l < 256; ++l) boundaries |= used[l] && (labels[l].type == LBF_PB || labels[l].type == LBF_VB);
 
-    int rc = setdev(e);
-    if (rc) { std::string m = e->last_error; lbf_destroy(e); return fail(nullptr, rc, m); }
-#define LBF_ALLOC(p, n)                                                  \
-    do {                                                                 \
-        int r_ = dalloc(e, &(p), (n));                                   \
-        if (r_) { std::string m_ = e->last_error; lbf_destroy(e); return fail(nullptr, r_, m_); } \
-    } while (0)
-#define LBF_CUDA(call)                                                   \
-    do {                                                                 \
-        cudaError_t r_ = (call);                                         \
-        if (r_ != cudaSuccess) { lbf_destroy(e); return fail(nullptr, LBF_ECUDA, std::string(#call) + ": " + cudaGetErrorString(r_)); } \
-    } while (0)
-    LBF_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
     const size_t fcount = (size_t)phases * e->Q * e->nfp;
     for (int b = 0; b < 2; ++b) {
         char* p = nullptr;
@@ -588,12 +721,31 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
             LBF_CUDA(cudaMemsetAsync(e->ex[b], 0, e->nfp, e->stream));
         }
     }
-    LBF_ALLOC(e->occ, occ.size());
     LBF_ALLOC(e->coord, e->nfp);
     LBF_ALLOC(e->label_force, 256 * 3);
-    LBF_CUDA(cudaMemcpyAsync(e->occ, occ.data(), occ.size() * sizeof(uint2), cudaMemcpyHostToDevice, e->stream));
-    LBF_CUDA(cudaMemcpyAsync(e->coord, coord.data(), coord.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, e->stream));
+    if (!uniform) LBF_ALLOC(e->node_label, e->nfp);
+    if (c.model == LBF_MODEL_COLOR) LBF_ALLOC(e->node_phase, e->nfp);
+    fill_nodes<<<cls_blocks, 256, 0, e->stream>>>(d_geom, e->occ, e->nx, e->ny, e->W, words, d_ltab + 256,
+                                                   e->coord, e->node_label, e->node_phase);
+    LBF_CUDA(cudaGetLastError());
     LBF_CUDA(cudaMemcpyAsync(e->label_force, lforce.data(), lforce.size() * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+    if (boundaries || c.model == LBF_MODEL_COLOR) {
+        if ((rc = ensure_vox(e))) { std::string m = e->last_error; lbf_destroy(e); return fail(nullptr, rc, m); }
+    }
+
+    // Zou-He boundary nodes in compact order (SCSP::zouHeBoundary, scsp.cpp:188-275).
+    std::vector<uint32_t> zh_node, zh_code;
+    std::vector<double> zh_value;
+    if (boundaries)
+        for (uint32_t k = 0; k < e->nf; ++k) {
+            const lbf_label& L = labels[geometry[e->vox[k]]];
+            if (L.type != LBF_PB && L.type != LBF_VB) continue;
+            zh_node.push_back(k);
+            zh_code.push_back(((uint32_t)L.phase << 16) | ((L.type == LBF_VB ? kZouHeVB : kZouHePB) << 8) |
+                              (uint32_t)L.dir);
+            zh_value.push_back(L.value);
+        }
+
     // Half-film bitmaps in the occupancy word layout (simulator.cpp:418-421).
     bool films = false;
     for (int l = 0; l < 256; ++l) films |= used[l] && labels[l].type == LBF_HF;
@@ -628,10 +780,6 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
         e->zh.code = e->zh_code;
         e->zh.value = e->zh_value;
     }
-    if (!uniform) {
-        LBF_ALLOC(e->node_label, e->nfp);
-        LBF_CUDA(cudaMemcpyAsync(e->node_label, nlabel.data(), nlabel.size(), cudaMemcpyHostToDevice, e->stream));
-    }
     LBF_ALLOC(e->rho0, e->nfp);
     LBF_ALLOC(e->u, 3 * (size_t)e->nfp);
     LBF_ALLOC(e->uprev, 3 * (size_t)e->nfp);
@@ -644,7 +792,6 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
     LBF_CUDA(cudaMemsetAsync(e->err, 0, sizeof(uint32_t), e->stream));
     LBF_ALLOC(e->partial, (size_t)kReduceBlocks * kReduceMaxK);
     LBF_ALLOC(e->red, kReduceMaxK);
-    LBF_CUDA(cudaMallocHost(&e->h_red, kReduceMaxK * sizeof(double)));
 
     e->force.uniform = uniform ? 1 : 0;
     e->force.fx = F0[0]; e->force.fy = F0[1]; e->force.fz = F0[2];
@@ -736,7 +883,6 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
         LBF_ALLOC(e->angle_id, e->nfp);
         LBF_ALLOC(e->angles, ang.size());
         LBF_ALLOC(e->tib, tib.size());
-        LBF_ALLOC(e->node_phase, e->nfp);
         LBF_CUDA(cudaMemsetAsync(e->rho1, 0, e->nfp * sizeof(double), e->stream));
         LBF_CUDA(cudaMemsetAsync(e->ind, 0, e->nfp * sizeof(double), e->stream));
         LBF_CUDA(cudaMemsetAsync(e->indprev, 0, e->nfp * sizeof(double), e->stream));
@@ -744,7 +890,6 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
         LBF_CUDA(cudaMemcpyAsync(e->angle_id, aid.data(), aid.size() * sizeof(uint16_t), cudaMemcpyHostToDevice, e->stream));
         LBF_CUDA(cudaMemcpyAsync(e->angles, ang.data(), ang.size() * sizeof(double), cudaMemcpyHostToDevice, e->stream));
         LBF_CUDA(cudaMemcpyAsync(e->tib, tib.data(), tib.size() * sizeof(double), cudaMemcpyHostToDevice, e->stream));
-        LBF_CUDA(cudaMemcpyAsync(e->node_phase, nphase.data(), nphase.size(), cudaMemcpyHostToDevice, e->stream));
         LBF_CUDA(cudaStreamSynchronize(e->stream));
     }
     LBF_CUDA(cudaStreamSynchronize(e->stream));
@@ -919,6 +1064,7 @@ int lbf_get_populations(lbf_engine* e, double* host, size_t n)
     if (n != need) return fail(e, LBF_EINVAL, "population buffer must hold phases*Q*N doubles");
     int rc = setdev(e);
     if (rc) return rc;
+    if ((rc = ensure_vox(e))) return rc;
     std::vector<double> compact;
     rc = expand_to_host(e, compact);
     if (rc) return rc;
@@ -939,6 +1085,7 @@ int lbf_set_populations(lbf_engine* e, const double* host, size_t n)
     if (n != need) return fail(e, LBF_EINVAL, "population buffer must hold phases*Q*N doubles");
     int rc = setdev(e);
     if (rc) return rc;
+    if ((rc = ensure_vox(e))) return rc;
     const size_t count = (size_t)e->phases * e->Q * e->nfp;
     std::vector<double> compact(count, 0.0);
     for (int p = 0; p < e->phases; ++p)
@@ -1032,6 +1179,7 @@ int lbf_get_macros(lbf_engine* e, double* rho0, double* rho1, double* u)
     if (!e) return fail(e, LBF_EINVAL, "NULL engine");
     int rc = setdev(e);
     if (rc) return rc;
+    if ((rc = ensure_vox(e))) return rc;
     std::vector<double> buf((size_t)e->nfp * 3);
     auto scatter = [&](const double* dsrc, double* dst, int comps) -> int {
         LBF_CK(e, cudaMemcpyAsync(buf.data(), dsrc, (size_t)comps * e->nfp * sizeof(double), cudaMemcpyDeviceToHost, e->stream));

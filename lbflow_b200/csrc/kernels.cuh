@@ -347,6 +347,7 @@ struct ScspParams {
     Trt rate;          // SRT: s+ = s- = 1/tau; MRT: legacy spectrum
     int mrt = 0;       // MRT: mass and momentum rows are not relaxed (rate 0)
     uint32_t seed = 0; // non-zero: stochastic rounding of 16-bit float storage (per-step seed)
+    uint32_t node0 = 0; // first node of the geometry: rounding streams follow the geometry's own node order
 };
 
 // Integer hash (lowbias32 of C. Wellons) seeding the per-node rounding stream.
@@ -426,7 +427,7 @@ __device__ __forceinline__ void scsp_update(const Grid& g, const Force& F, const
         if (P.seed) {
             // One linear congruential stream per node and step; its high bits
             // are the rounding offsets.
-            uint32_t r = hash32(i * 0x9e3779b9u + P.seed);
+            uint32_t r = hash32((i - P.node0) * 0x9e3779b9u + P.seed);
 #pragma unroll
             for (int q = 0; q < L::Q; ++q) {
                 r = r * 1664525u + 1013904223u;

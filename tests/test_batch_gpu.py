@@ -35,8 +35,10 @@ def _engine_fields(g, tau, steps, storage='fp64'):
         return r, u, e.flux_sums()
 
 
-@pytest.mark.parametrize('storage', ['fp64', 'fp32'])
+@pytest.mark.parametrize('storage', ['fp64', 'fp32', 'fp16'])
 def test_batch_matches_single_engines_bitwise(storage):
+    """FP16 included: its stochastic rounding takes the same per-step seeds
+    and per-node streams as the single engine, also inside graph replays."""
     from lbflow_b200.batch import Batch
     geoms, taus = _geometries()
     steps = 150   # exercises graph replays (64-step graphs) and explicit steps
