@@ -318,6 +318,11 @@ def main():
                                                   'warmstart.pt'), help='ttp: trained warm-start operator')
     ap.add_argument('--check', type=int, default=8, help='batch: geometries re-solved alone in FP64')
     ap.add_argument('--ref-steps', type=int, default=3, help='reference arm: steps per reference process')
+    ap.add_argument('--no-ttp', action='store_true', help='default line without the time-to-permeability runs')
+    ap.add_argument('--ttp-runs', default='fp64,fp16+acc,fp16+mob,fp16+mob+acc',
+                    help='runs of the default line\'s time-to-permeability object')
+    ap.add_argument('--mob-weights', default=str(Path(__file__).resolve().parent / 'lbflow_b200' / 'weights' /
+                                                 'mobility.pt'), help='trained block-mobility operator')
     ap.add_argument('--ref-procs', type=int, default=None, help='reference arm: cap on concurrent processes')
     args = ap.parse_args()
     if args.warmup < 3:
@@ -396,6 +401,10 @@ def main():
         eng.close()
         e2e = end_to_end(geometry, args, local)
 
+    ttp = None
+    if rank == 0 and world == 1 and not args.no_ttp and args.storage == 'fp64' and args.size % 8 == 0:
+        ttp = ttp_line(args)
+
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base, _ = reference_sample(steps=2, procs=1)
@@ -416,7 +425,7 @@ def main():
                                   frac=achieved / peak, traffic=traffic, peak_kind=peak_kind,
                                   bytes_per_launch=bytes_launch, launch_ms=launch_ms),
                     gpu_launches=args.steps,
-                    clocks=clk, e2e=e2e, cpu_baseline=base)
+                    clocks=clk, e2e=e2e, cpu_baseline=base, ttp=ttp)
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
@@ -623,6 +632,97 @@ def ttp_media(args):
     return out
 
 
+def ttp_medium(med, args, net, storages):
+    """Time-to-permeability runs of one medium; returns (runs, histories)."""
+    import torch
+    from lbflow_b200 import Engine
+    from lbflow_b200 import warmstart as ws
+    from lbflow_b200.permeability import converge
+    geometry = med['geometry']
+    fluid = torch.from_numpy(geometry != 255).cuda()
+    names = storages.split(',')
+    # One-time set-up outside the timed runs, as CUDA context creation is:
+    # CUDA kernels (the library's and torch's size-dependent variants) load
+    # on first launch, so a throwaway engine of each storage takes one step,
+    # one block correction and, for warm starts, one network inference on
+    # this medium.  No state carries over into the timed runs.
+    for storage in sorted({n.split('+')[0] for n in names}):
+        with Engine(geometry, LABELS, model='scsp', collision=args.collision, tau=(1.0,), rho=(1.0,),
+                    storage=storage) as e:
+            e.initialize()
+            e.step(1, macros=True)
+            if any('+acc' in n for n in names):
+                ws.DarcyAccelerator(e, fluid, 1e-5, block=args.block, at=(1,))(1)
+            if net is not None:
+                ws.predict(net, fluid, 1.0, 1e-5)
+            if any('+mob' in n for n in names):
+                ws.mobility_start(e, args.mob_net, fluid, 1.0, 1e-5, block=args.block)
+            e.check()
+    torch.cuda.synchronize()
+    runs, hist = {}, {}
+    for name in names:
+        storage, *mods = name.split('+')
+        start = acc = None
+        eng = Engine(geometry, LABELS, model='scsp', collision=args.collision, tau=(1.0,), rho=(1.0,),
+                     storage=storage)
+        for mod in mods:
+            kind = mod.rstrip('0123456789')
+            block = int(mod[len(kind):]) if mod[len(kind):] else args.block
+            if kind in ('warm', 'warmv', 'flux', 'rho'):
+                mode = {'warm': 'darcy', 'warmv': 'darcy', 'flux': 'flux', 'rho': 'none'}[kind] if block else 'none'
+                start = (lambda b=block, m=mode, v=(kind == 'warmv'):
+                         ws.warm_start(eng, net, fluid, 1.0, 1e-5, block=b, mode=m, velocity=v))
+            elif kind == 'mob':
+                start = (lambda b=block: ws.mobility_start(eng, args.mob_net, fluid, 1.0, 1e-5, block=b))
+            elif kind == 'acc':
+                sched = [tuple(int(v) for v in item.split(':')) if ':' in item else int(item)
+                         for item in args.accel_at.split(',')]
+                acc = ws.DarcyAccelerator(eng, fluid, 1e-5, block=block, at=sched, face=args.accel_face,
+                                          omega=args.accel_omega)
+        r = converge(eng, 1.0, 1e-5, report=args.report, tol=1e-6, max_steps=args.max_steps, warm=start,
+                     accelerate=acc)
+        hist[name] = r['history']
+        runs[name] = dict(steps=r['steps'], seconds=r['seconds'], K=r['K'], converged=r['converged'],
+                          fallback=r['fallback'], fluid_nodes=eng.fluid_nodes,
+                          mlups=eng.fluid_nodes * r['steps'] / r['seconds'] / 1e6)
+        if acc is not None:
+            runs[name]['accelerator'] = dict(applied=acc.applied, seconds=acc.seconds,
+                                             cg_iterations=acc.iterations, phases=acc.phases)
+        if args.history:
+            runs[name]['history'] = [(h[0], h[1], h[3]) for h in r['history']]
+        eng.close()
+    return runs, hist
+
+
+def band_summary(runs, hist, k_ref):
+    """Adds K error, steps/seconds to the 1e-3 band and speed-ups against fp64."""
+    from lbflow_b200.permeability import time_to_band
+    base = runs.get('fp64')
+    for k, v in runs.items():
+        if k_ref:
+            v['K_rel_error_vs_fp64'] = abs(v['K'] - k_ref) / abs(k_ref)
+            band = time_to_band(hist[k], k_ref, 1e-3)
+            v['to_1e-3_band'] = dict(steps=band[0], seconds=band[1]) if band else None
+        if base:
+            v['speedup_vs_fp64'] = base['seconds'] / v['seconds']
+    if base and base.get('to_1e-3_band'):
+        b0 = base['to_1e-3_band']['seconds']
+        for k, v in runs.items():
+            if v.get('to_1e-3_band'):
+                v['to_1e-3_band']['speedup_vs_fp64'] = b0 / v['to_1e-3_band']['seconds']
+
+
+def load_networks(args, storages):
+    from lbflow_b200 import warmstart as ws
+    net = None
+    if any(m in r for r in storages.split(',') for m in ('+warm', '+flux', '+rho')):
+        net, _ = ws.load(args.warm_weights)
+    args.mob_net = None
+    if '+mob' in storages:
+        args.mob_net, _ = ws.load_mobility(args.mob_weights)
+    return net
+
+
 def time_to_permeability(args):
     """Wall time to LBFlow's convergence criterion (report every --report
     steps, relative velocity change < 1e-6 three times in a row) and to K within 1e-3
@@ -633,83 +733,20 @@ def time_to_permeability(args):
     blocks, inside the timed region); '+warmB' sets the block edge B (0: the
     network's fields only); '+fluxB' uses the flux-divergence correction
     instead; warm starts set the predicted density only ('+warmvB' also the
-    predicted velocity);
-    '+accB' applies the in-run block Darcy correction
-    (warmstart.DarcyAccelerator) at the --accel-at report steps.
-    K = nu <u_x> / g."""
+    predicted velocity); '+mobB' starts from the block Darcy pressure of the
+    learned block mobilities (warmstart.mobility_start); '+accB' applies the
+    in-run block Darcy correction (warmstart.DarcyAccelerator) at the
+    --accel-at report steps.  K = nu <u_x> / g."""
     import torch
-    from lbflow_b200 import Engine
-    from lbflow_b200.permeability import converge, time_to_band
     torch.cuda.set_device(0)
-    net = None
-    from lbflow_b200 import warmstart as ws
-    if any(m in r for r in args.storages.split(',') for m in ('+warm', '+flux', '+rho')):
-        net, wmeta = ws.load(args.warm_weights)
+    net = load_networks(args, args.storages)
     media = ttp_media(args)
     results = []
     for med in media:
-        geometry = med['geometry']
-        fluid = torch.from_numpy(geometry != 255).cuda()
-        # One-time set-up outside the timed runs, as CUDA context creation is:
-        # CUDA kernels (the library's and torch's size-dependent variants) load
-        # on first launch, so a throwaway engine of each storage takes one step,
-        # one block correction and, for warm starts, one network inference on
-        # this medium.  No state carries over into the timed runs.
-        for storage in sorted({n.split('+')[0] for n in args.storages.split(',')}):
-            with Engine(geometry, LABELS, model='scsp', collision=args.collision, tau=(1.0,), rho=(1.0,),
-                        storage=storage) as e:
-                e.initialize()
-                e.step(1, macros=True)
-                if any('+acc' in n for n in args.storages.split(',')):
-                    ws.DarcyAccelerator(e, fluid, 1e-5, block=args.block, at=(1,))(1)
-                if net is not None:
-                    ws.predict(net, fluid, 1.0, 1e-5)
-                e.check()
-        torch.cuda.synchronize()
-        runs, hist = {}, {}
-        for name in args.storages.split(','):
-            storage, *mods = name.split('+')
-            start = acc = None
-            eng = Engine(geometry, LABELS, model='scsp', collision=args.collision, tau=(1.0,), rho=(1.0,),
-                         storage=storage)
-            for mod in mods:
-                kind = mod.rstrip('0123456789')
-                block = int(mod[len(kind):]) if mod[len(kind):] else args.block
-                if kind in ('warm', 'warmv', 'flux', 'rho'):
-                    mode = {'warm': 'darcy', 'warmv': 'darcy', 'flux': 'flux', 'rho': 'none'}[kind] if block else 'none'
-                    start = (lambda b=block, m=mode, v=(kind == 'warmv'):
-                             ws.warm_start(eng, net, fluid, 1.0, 1e-5, block=b, mode=m, velocity=v))
-                elif kind == 'acc':
-                    sched = [tuple(int(v) for v in item.split(':')) if ':' in item else int(item)
-                             for item in args.accel_at.split(',')]
-                    acc = ws.DarcyAccelerator(eng, fluid, 1e-5, block=block, at=sched, face=args.accel_face,
-                                              omega=args.accel_omega)
-            r = converge(eng, 1.0, 1e-5, report=args.report, tol=1e-6, max_steps=args.max_steps, warm=start,
-                         accelerate=acc)
-            hist[name] = r['history']
-            runs[name] = dict(steps=r['steps'], seconds=r['seconds'], K=r['K'], converged=r['converged'],
-                              fallback=r['fallback'], fluid_nodes=eng.fluid_nodes,
-                              mlups=eng.fluid_nodes * r['steps'] / r['seconds'] / 1e6)
-            if acc is not None:
-                runs[name]['accelerator'] = dict(applied=acc.applied, seconds=acc.seconds,
-                                                 cg_iterations=acc.iterations, phases=acc.phases)
-            if args.history:
-                runs[name]['history'] = [(h[0], h[1], h[3]) for h in r['history']]
-            eng.close()
+        runs, hist = ttp_medium(med, args, net, args.storages)
         base = runs.get('fp64')
         kref = args.k_ref if args.k_ref else (base['K'] if base else None)
-        for k, v in runs.items():
-            if kref:
-                v['K_rel_error_vs_fp64'] = abs(v['K'] - kref) / abs(kref)
-                band = time_to_band(hist[k], kref, 1e-3)
-                v['to_1e-3_band'] = dict(steps=band[0], seconds=band[1]) if band else None
-            if base:
-                v['speedup_vs_fp64'] = base['seconds'] / v['seconds']
-        if base and runs['fp64'].get('to_1e-3_band'):
-            b0 = runs['fp64']['to_1e-3_band']['seconds']
-            for k, v in runs.items():
-                if v.get('to_1e-3_band'):
-                    v['to_1e-3_band']['speedup_vs_fp64'] = b0 / v['to_1e-3_band']['seconds']
+        band_summary(runs, hist, kref)
         results.append(dict(medium=med['name'], sigma=med['sigma'], porosity=med['porosity'], seed=med['seed'],
                             runs=runs))
         print(json.dumps(results[-1]), flush=True)
@@ -718,8 +755,10 @@ def time_to_permeability(args):
         sp = [r['runs'][name]['to_1e-3_band']['speedup_vs_fp64'] for r in results
               if r['runs'][name].get('to_1e-3_band') and 'speedup_vs_fp64' in r['runs'][name]['to_1e-3_band']]
         ke = [r['runs'][name].get('K_rel_error_vs_fp64') for r in results if 'K_rel_error_vs_fp64' in r['runs'][name]]
+        st = [r['runs'][name]['to_1e-3_band']['steps'] for r in results if r['runs'][name].get('to_1e-3_band')]
         summary[name] = dict(band_speedup_median=float(np.median(sp)) if sp else None,
                              band_speedup_min=float(min(sp)) if sp else None,
+                             band_steps_median=float(np.median(st)) if st else None,
                              K_rel_error_max=float(max(ke)) if ke else None,
                              fallbacks=sum(bool(r['runs'][name]['fallback']) for r in results))
     print(json.dumps(dict(metric='time to permeability (K within 1e-3 of converged FP64; 1e-6 convergence)',
@@ -728,6 +767,29 @@ def time_to_permeability(args):
                           summary=summary)))
     return 0
 
+
+def ttp_line(args):
+    """The time-to-permeability sub-object of the default line: the 256^3
+    cube of the throughput workload, FP64 from rest (LBFlow's method; its
+    converged K is the reference) against the chosen forms."""
+    net = load_networks(args, args.ttp_runs)
+    med = ttp_media(argparse.Namespace(ttp_media='cube', size=args.size))[0]
+    runs, hist = ttp_medium(med, args, net, args.ttp_runs)
+    k_ref = runs['fp64']['K'] if runs.get('fp64', {}).get('converged') else None
+    band_summary(runs, hist, k_ref)
+    slim = {}
+    for name, v in runs.items():
+        b = v.get('to_1e-3_band') or {}
+        slim[name] = dict(steps_to_band=b.get('steps'), seconds_to_band=b.get('seconds'),
+                          band_speedup_vs_fp64=b.get('speedup_vs_fp64'), converged=v['converged'],
+                          steps_to_converge=v['steps'], seconds_to_converge=v['seconds'], K=v['K'],
+                          K_rel_error_vs_fp64=v.get('K_rel_error_vs_fp64'), fallback=v['fallback'])
+        if 'accelerator' in v:
+            slim[name]['correction_seconds'] = v['accelerator']['seconds']
+    return dict(metric='time to permeability within 1e-3 of the converged FP64 K (wall seconds)',
+                medium=f'{args.size}^3 cube, sigma 3, porosity 0.22, seed 0', report_interval=args.report,
+                convergence='LBFlow criterion: relative velocity change < 1e-6 at 3 consecutive reports',
+                K_ref=k_ref, runs=slim)
 
 
 def operator_run(args):

@@ -187,7 +187,10 @@ int lbf_get_macros(lbf_engine *e, double *rho0, double *rho1, double *u);
  * waits).  `out` must be memory the device can write: device memory of the
  * engine's device, or page-locked host memory (lbf_host_alloc, or any
  * cudaHostAlloc/cudaHostRegister memory); pageable memory is refused.  Keep
- * it alive and unread until the wait returns.
+ * it alive and unread until the wait returns.  Device memory is written in
+ * place; page-locked host memory is filled by DMA copies from a 256 MiB
+ * device staging buffer that the first such call allocates and the engine
+ * keeps.
  *
  * lbf_fields_dense_async replaces the field gathering of FileVti::Save
  * (filevti.cpp:113-172): out holds, for N = nx*ny*nz voxels, rho0 [N], then

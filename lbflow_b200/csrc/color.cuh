@@ -62,8 +62,32 @@ __device__ __forceinline__ void color_gather(const Grid& g, const Film& film, co
                                              typename S::R (&f1)[L::Q], uint32_t (&nbr)[L::Q])
 {
     using R = typename S::R;
-    gather<L, S, PULL>(g, fin, i, x, y, z, f0, nbr, R(0));
-    gather<L, S, PULL>(g, fin + (size_t)L::Q * g.nfp, i, x, y, z, f1, nbr, R(0));
+    // One neighbour lookup for both components (the sources are the same).
+    const typename S::T* __restrict__ fin1 = fin + (size_t)L::Q * g.nfp;
+    const uint32_t nfp = g.nfp;
+    f0[0] = S::load(fin + i, 0, R(0));
+    f1[0] = S::load(fin1 + i, 0, R(0));
+    nbr[0] = i;
+    if constexpr (!PULL) {
+#pragma unroll
+        for (int q = 1; q < L::Q; ++q) {
+            f0[q] = S::load(fin + (q * nfp + i), q, R(0));
+            f1[q] = S::load(fin1 + (q * nfp + i), q, R(0));
+            nbr[q] = 0;
+        }
+    } else {
+        uint32_t src[L::Q];
+        const uint32_t mask = pull_sources<L>(g, x, y, z, src);
+#pragma unroll
+        for (int q = 1; q < L::Q; ++q) {
+            const bool fluid = (mask >> q) & 1u;
+            const uint32_t node = fluid ? src[q] : i;
+            nbr[L::op(q)] = fluid ? src[q] : 0xffffffffu;
+            const uint32_t off = (fluid ? (uint32_t)q : (uint32_t)L::op(q)) * nfp + node;
+            f0[q] = S::load(fin + off, q, R(0));
+            f1[q] = S::load(fin1 + off, q, R(0));
+        }
+    }
     if constexpr (FILM && PULL) {
         const uint32_t b1 = film_sources<L>(g, film.bits[1], x, y, z);   // blocks phase 0
         const uint32_t b0 = film_sources<L>(g, film.bits[0], x, y, z);   // blocks phase 1
@@ -140,9 +164,14 @@ __device__ __forceinline__ void color_update(const Grid& g, const Force& F, cons
 {
     using R = typename S::R;
     // ColorFluid::calcMacroVar (colorfluid.cpp:238-290) and bodyForce (:736-750).
+    // The total distribution fT = f0 + f1 is formed first; afterwards only
+    // fT and the two component densities stay live (register budget).
     R d0 = f0[0], d1 = f1[0];
 #pragma unroll
     for (int q = 1; q < L::Q; ++q) { d0 += f0[q]; d1 += f1[q]; }
+    R fT[L::Q];
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) fT[q] = f0[q] + f1[q];
     const R dt = d0 + d1;
     const R phi_i = (d0 - d1) / dt;
     const R tau = (R(1) + phi_i) * R(P.relax0) + (R(1) - phi_i) * R(P.relax1);
@@ -161,8 +190,8 @@ __device__ __forceinline__ void color_update(const Grid& g, const Force& F, cons
 #pragma unroll
         for (int q = 1; q < L::Q; ++q) {
             const int e = comp<L>(q, a);
-            if (e == 1) v += f0[q] + f1[q];
-            else if (e == -1) v -= f0[q] + f1[q];
+            if (e == 1) v += fT[q];
+            else if (e == -1) v -= fT[q];
         }
         u[a] = v / dt;
     }
@@ -183,36 +212,13 @@ __device__ __forceinline__ void color_update(const Grid& g, const Force& F, cons
         for (int a = 0; a < 3; ++a) mo.uadj[(size_t)a * g.nfp + i] = (double)u[a];
     }
 
-    // ColorFluid::collision (colorfluid.cpp:334-387): collide the total
-    // fT = f0 + f1 towards feq = feq_u0 + rho w (3 e.u + 4.5 (e.u)^2 - 1.5 u^2),
-    // feq_u0 = rho0 ai0 + rho1 ai1, with the same two-rate form as the
-    // single-phase step: SRT is s+ = s- = 1/tau_local; MRT uses the tau0 rates
-    // when tau0 == tau1 and getMRTS(tau_local) otherwise (simulator.cpp:199-216).
-    const R usq = u[2] * u[2] + u[1] * u[1] + u[0] * u[0];
-    const R uf = u[2] * Fv[2] + u[1] * Fv[1] + u[0] * Fv[0];
-    R fT[L::Q], fu0[L::Q];
-#pragma unroll
-    for (int q = 0; q < L::Q; ++q) {
-        fT[q] = f0[q] + f1[q];
-        fu0[q] = d0 * R(P.ai[0][q]) + d1 * R(P.ai[1][q]);
-    }
-    R sp, sm;
-    if (COLL == 0) {
-        sp = sm = R(1) / tau;
-    } else if (P.uniform_tau) {
-        sp = R(P.rate.sp);
-        sm = R(P.rate.sm);
-    } else {
-        sp = R(1) / tau;
-        sm = R(8) * (R(2) - sp) / (R(8) - sp);
-    }
-    collide_trt<L, R, true>(fT, fu0, -dt * R(1.5) * usq, dt * R(4.5), dt * R(3), u, Fv, uf, sp, sm);
-
     // ColorFluid::colorGradient (colorfluid.cpp:435-570), gradient in the
-    // reference component order gr[0..D-1] = {z,y,x} / {y,x}.  The gradient
-    // and the wall rotation use non-contracted IEEE operations in the
-    // reference's order: the rotation angle is undefined when the in-plane
-    // gradient vanishes, so exact cancellations must stay exact.
+    // reference component order gr[0..D-1] = {z,y,x} / {y,x}; it only needs
+    // the neighbours' phase field, so it is done before the collision and
+    // the neighbour data is dead by then.  The gradient and the wall rotation
+    // use non-contracted IEEE operations in the reference's order: the
+    // rotation angle is undefined when the in-plane gradient vanishes, so
+    // exact cancellations must stay exact.
     R gr[3] = {R(0), R(0), R(0)};
     const uint16_t wid = __ldg(&W.angle_id[i]);
     R phin[L::Q];
@@ -298,6 +304,33 @@ __device__ __forceinline__ void color_update(const Grid& g, const Force& F, cons
         }
     }
 
+    // ColorFluid::collision (colorfluid.cpp:334-387): collide the total
+    // fT towards feq = feq_u0 + rho w (3 e.u + 4.5 (e.u)^2 - 1.5 u^2),
+    // feq_u0 = rho0 ai0 + rho1 ai1, with the same two-rate form as the
+    // single-phase step: SRT is s+ = s- = 1/tau_local; MRT uses the tau0 rates
+    // when tau0 == tau1 and getMRTS(tau_local) otherwise (simulator.cpp:199-216).
+    // ai_k,q takes one value per direction class (rest, axis, diagonal), so
+    // feq_u0 is formed once per class.
+    const R usq = u[2] * u[2] + u[1] * u[1] + u[0] * u[0];
+    const R uf = u[2] * Fv[2] + u[1] * Fv[1] + u[0] * Fv[0];
+    constexpr int kDiag = L::D == 3 ? 7 : 5;
+    const R fuc[3] = {d0 * R(P.ai[0][0]) + d1 * R(P.ai[1][0]), d0 * R(P.ai[0][1]) + d1 * R(P.ai[1][1]),
+                      d0 * R(P.ai[0][kDiag]) + d1 * R(P.ai[1][kDiag])};
+    R fu0[L::Q];
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) fu0[q] = fuc[q == 0 ? 0 : (axis_dir<L>(q) ? 1 : 2)];
+    R sp, sm;
+    if (COLL == 0) {
+        sp = sm = R(1) / tau;
+    } else if (P.uniform_tau) {
+        sp = R(P.rate.sp);
+        sm = R(P.rate.sm);
+    } else {
+        sp = R(1) / tau;
+        sm = R(8) * (R(2) - sp) / (R(8) - sp);
+    }
+    collide_trt<L, R, true>(fT, fu0, -dt * R(1.5) * usq, dt * R(4.5), dt * R(3), u, Fv, uf, sp, sm);
+
     // Perturbation and cosine recoloring (colorfluid.cpp:399-428).
     const R dens0T = d0 / dt;
     typename S::T* o0 = fout;
@@ -333,14 +366,21 @@ __device__ __forceinline__ void color_update(const Grid& g, const Force& F, cons
 
 // Pass 2: collision, gradient, perturbation and recoloring of every fluid node.
 // PULL = false is the t = 0 collision.
+// At most 128 registers per thread (four 128-thread blocks per SM): the
+// kernel is latency-bound, and the FP64 D3Q19 form otherwise needs 132
+// registers, which leaves three blocks per SM (measured 12 % slower).
 template <class L, class S, int COLL, bool PULL, bool FILM>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 4)
 color_collide(const Grid g, const Film film, const Force F, const ColorParams P, const ColorWall W,
               const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
               const double* __restrict__ phi, Macros mo, const int out, uint32_t* __restrict__ err)
 {
     using R = typename S::R;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    // Blocks run in descending node order: pass 1 has just read the
+    // populations in ascending order, so the highest nodes' lines are the
+    // ones still in L2, and the next step's pass 1 starts with the lowest
+    // nodes, the last ones written here.
+    const uint32_t i = (gridDim.x - 1 - blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= g.nf) return;
     int x, y, z;
     unpack(__ldg(&g.coord[i]), x, y, z);

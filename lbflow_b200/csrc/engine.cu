@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <new>
 #include <string>
 #include <utility>
@@ -42,6 +43,7 @@ struct lbf_engine {
     uint32_t* err = nullptr;
     double* partial = nullptr;
     double* dense_tmp = nullptr;    // FP64 copy of reduced-precision populations (dense output)
+    double* stage = nullptr;        // device staging of dense outputs bound for host memory
     double* red = nullptr;
     double* h_red = nullptr;        // pinned
     cudaStream_t stream = nullptr;
@@ -54,6 +56,7 @@ struct lbf_engine {
     ColorParams cp{};
     bool initialized = false;
     uint32_t steps = 0;             // pull steps launched (seeds the 16-bit stochastic rounding)
+    uint32_t pulls = 0;             // pull steps launched (alternates the step kernel's node order)
     uint64_t bytes = 0;
     std::string last_error;
 };
@@ -76,12 +79,46 @@ int fail(lbf_engine* e, int code, const std::string& msg)
             return fail(e, LBF_ECUDA, std::string(#call) + ": " + cudaGetErrorString(err_)); \
     } while (0)
 
+// Engine state comes from one stream-ordered memory pool per device that
+// keeps up to kPoolKeepBytes reserved after frees, so that destroying an
+// engine and creating the next one (a sequence of runs, or a run after a
+// throwaway warm-up engine) reuses mapped device memory instead of mapping
+// gigabytes again; larger reservations are returned to the driver when a
+// stream synchronises.
+constexpr uint64_t kPoolKeepBytes = 8ull << 30;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[64] = {};
+
+cudaError_t engine_pool(int device, cudaMemPool_t* pool)
+{
+    if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (!g_pool[device]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t p = nullptr;
+        cudaError_t r = cudaMemPoolCreate(&p, &props);
+        if (r != cudaSuccess) return r;
+        uint64_t keep = kPoolKeepBytes;
+        r = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (r != cudaSuccess) { cudaMemPoolDestroy(p); return r; }
+        g_pool[device] = p;
+    }
+    *pool = g_pool[device];
+    return cudaSuccess;
+}
+
 template <class T>
 int dalloc(lbf_engine* e, T** p, size_t count)
 {
     *p = nullptr;
     if (count == 0) count = 1;
-    cudaError_t r = cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T));
+    cudaMemPool_t pool = nullptr;
+    cudaError_t r = engine_pool(e->cfg.device, &pool);
+    if (r == cudaSuccess)
+        r = cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), count * sizeof(T), pool, e->stream);
     if (r != cudaSuccess)
         return fail(e, r == cudaErrorMemoryAllocation ? LBF_ENOMEM : LBF_ECUDA,
                     std::string("cudaMalloc: ") + cudaGetErrorString(r));
@@ -185,6 +222,7 @@ void launch_step(lbf_engine* e, bool pull, int out)
         // nearest.
         const bool dither = e->cfg.storage == LBF_STORE_FP16 || e->cfg.storage == LBF_STORE_BF16;
         e->sp.seed = dither && pull ? (++e->steps * 2654435761u) | 1u : 0u;
+        e->sp.reverse = pull ? (int)(++e->pulls & 1u) : 0;
         ScspLaunch a{grid_of(e), e->force, e->sp, fin, fout, macros_of(e), e->err, e->stream,
                      e->ex[e->cur], e->ex[e->cur ^ 1], out};
         launch_scsp(e->D, (int)e->cfg.storage, e->cfg.collision == LBF_MRT, pull, out, a);
@@ -365,33 +403,38 @@ void set_global_error(const std::string& msg) { g_create_error = msg; }
 }  // namespace lbf
 
 namespace {
-// Dense outputs, one thread per voxel (grid-stride), x fastest, so that a
-// warp writes consecutive addresses of every array.
-__global__ void fields_dense_kernel(const lbf::Grid g, const double* __restrict__ rho0,
+// Dense outputs of voxels [v0, v0 + r), one thread per voxel (grid-stride),
+// x fastest, so that a warp writes consecutive addresses of every array.
+// Fields: out = [rho0 r][rho1 r (color)][velocity r x D interleaved];
+// populations: out = [block][r].  With v0 = 0 and r = N these are the file
+// layouts themselves.
+__global__ void fields_range_kernel(const lbf::Grid g, const double* __restrict__ rho0,
                                     const double* __restrict__ rho1, const double* __restrict__ u, int D,
-                                    double* __restrict__ out, size_t N)
+                                    size_t v0, size_t r, double* __restrict__ out)
 {
-    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < N; v += (size_t)gridDim.x * blockDim.x) {
+    for (size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x; j < r; j += (size_t)gridDim.x * blockDim.x) {
+        const size_t v = v0 + j;
         const int x = (int)(v % g.nx);
         const int y = (int)((v / g.nx) % g.ny);
         const int z = (int)(v / ((size_t)g.nx * g.ny));
         bool fluid;
         const uint32_t k = lbf::lookup(g, x, y, z, fluid);
-        out[v] = fluid ? rho0[k] : 0.0;
-        size_t o = N;
+        out[j] = fluid ? rho0[k] : 0.0;
+        size_t o = r;
         if (rho1) {
-            out[N + v] = fluid ? rho1[k] : 0.0;
-            o += N;
+            out[r + j] = fluid ? rho1[k] : 0.0;
+            o += r;
         }
-        for (int c = 0; c < D; ++c) out[o + v * D + c] = fluid ? u[(size_t)c * g.nfp + k] : 0.0;
+        for (int c = 0; c < D; ++c) out[o + j * D + c] = fluid ? u[(size_t)c * g.nfp + k] : 0.0;
     }
 }
 
-__global__ void populations_dense_kernel(const lbf::Grid g, const double* __restrict__ in, int blocks,
-                                         double* __restrict__ out, size_t N, uint32_t* __restrict__ err)
+__global__ void populations_range_kernel(const lbf::Grid g, const double* __restrict__ in, int blocks, size_t v0,
+                                         size_t r, double* __restrict__ out, uint32_t* __restrict__ err)
 {
     bool bad = false;
-    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < N; v += (size_t)gridDim.x * blockDim.x) {
+    for (size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x; j < r; j += (size_t)gridDim.x * blockDim.x) {
+        const size_t v = v0 + j;
         const int x = (int)(v % g.nx);
         const int y = (int)((v / g.nx) % g.ny);
         const int z = (int)(v / ((size_t)g.nx * g.ny));
@@ -400,25 +443,40 @@ __global__ void populations_dense_kernel(const lbf::Grid g, const double* __rest
         for (int b = 0; b < blocks; ++b) {
             const double val = fluid ? in[(size_t)b * g.nfp + k] : 0.0;
             bad |= !isfinite(val);
-            out[(size_t)b * N + v] = val;
+            out[(size_t)b * r + j] = val;
         }
     }
     if (bad) atomicOr(err, lbf::kErrOutput);
 }
 
-// The device address of a caller buffer, or nullptr when the device cannot
-// write it (pageable host memory, another device's memory).
-double* device_writable(lbf_engine* e, double* p)
+// Where a dense output goes: device memory of the engine's device or managed
+// memory (written in place by the kernel), or page-locked host memory (written
+// through a device staging buffer and copied by DMA: direct kernel stores to
+// host memory cross PCIe as small transactions and run several times slower).
+enum class Dest { kNone, kDevice, kHost };
+Dest destination(lbf_engine* e, double* p)
 {
     cudaPointerAttributes pa{};
     if (cudaPointerGetAttributes(&pa, p) != cudaSuccess) {
         cudaGetLastError();
-        return nullptr;
+        return Dest::kNone;
     }
-    if (pa.type == cudaMemoryTypeDevice) return pa.device == e->cfg.device ? p : nullptr;
-    if (pa.type == cudaMemoryTypeManaged) return p;
-    if (pa.type == cudaMemoryTypeHost) return static_cast<double*>(pa.devicePointer);
-    return nullptr;
+    if (pa.type == cudaMemoryTypeDevice) return pa.device == e->cfg.device ? Dest::kDevice : Dest::kNone;
+    if (pa.type == cudaMemoryTypeManaged) return Dest::kDevice;
+    if (pa.type == cudaMemoryTypeHost) return Dest::kHost;
+    return Dest::kNone;
+}
+
+// Device staging buffer for host destinations (allocated on first use, kept).
+constexpr size_t kStageBytes = (size_t)256 << 20;
+int stage_buffer(lbf_engine* e, double** out)
+{
+    if (!e->stage) {
+        const int rc = dalloc(e, &e->stage, kStageBytes / sizeof(double));
+        if (rc) return rc;
+    }
+    *out = e->stage;
+    return LBF_OK;
 }
 
 unsigned dense_blocks(size_t N)
@@ -630,10 +688,14 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
                                   (int64_t)words);
     struct Scratch {
         void* p[4] = {nullptr, nullptr, nullptr, nullptr};
-        ~Scratch() { for (void* q : p) if (q) cudaFree(q); }
+        cudaStream_t s = nullptr;
+        ~Scratch() { for (void* q : p) if (q) cudaFreeAsync(q, s); }
     } scratch;
+    scratch.s = e->stream;
+    cudaMemPool_t pool = nullptr;
+    LBF_CUDA(engine_pool((int)c.device, &pool));
     auto salloc = [&](void** p, size_t bytes, int slot) -> cudaError_t {
-        const cudaError_t r = cudaMalloc(p, bytes ? bytes : 1);
+        const cudaError_t r = cudaMallocFromPoolAsync(p, bytes ? bytes : 1, pool, e->stream);
         if (r == cudaSuccess) scratch.p[slot] = *p;
         return r;
     };
@@ -907,8 +969,10 @@ void lbf_destroy(lbf_engine* e)
     void* ptrs[] = {e->f[0], e->f[1], e->ex[0], e->ex[1], e->occ, e->coord, e->node_label, e->node_phase, e->label_force,
                     e->rho0, e->rho1, e->u, e->uprev, e->uadj, e->ind, e->indprev, e->indadj,
                     e->phi, e->angle_id, e->angles, e->tib, e->err, e->partial, e->red,
-                    e->zh_node, e->zh_code, e->zh_value, e->zh_num, e->dense_tmp, e->film_bits[0], e->film_bits[1]};
-    for (void* p : ptrs) if (p) cudaFree(p);
+                    e->zh_node, e->zh_code, e->zh_value, e->zh_num, e->dense_tmp, e->film_bits[0], e->film_bits[1],
+                    e->stage};
+    for (void* p : ptrs) if (p) cudaFreeAsync(p, e->stream);
+    if (e->stream) cudaStreamSynchronize(e->stream);
     if (e->h_red) cudaFreeHost(e->h_red);
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
@@ -1119,16 +1183,36 @@ int lbf_fields_dense_async(lbf_engine* e, double* out, size_t n)
 {
     if (!e || !out) return fail(e, LBF_EINVAL, "NULL argument");
     const bool color = e->cfg.model == LBF_MODEL_COLOR;
-    if (n != (size_t)(1 + (color ? 1 : 0) + e->D) * e->N)
+    const int per = 1 + (color ? 1 : 0) + e->D;
+    if (n != (size_t)per * e->N)
         return fail(e, LBF_EINVAL, "fields buffer must hold (1 + color + dims) * nx*ny*nz doubles");
     int rc = setdev(e);
     if (rc) return rc;
-    double* d = device_writable(e, out);
-    if (!d) return fail(e, LBF_EINVAL, "out must be device memory of the engine's device or page-locked host memory");
+    const Dest dst = destination(e, out);
+    if (dst == Dest::kNone)
+        return fail(e, LBF_EINVAL, "out must be device memory of the engine's device or page-locked host memory");
     if (e->N == 0) return LBF_OK;
-    fields_dense_kernel<<<dense_blocks(e->N), 256, 0, e->stream>>>(grid_of(e), e->rho0, color ? e->rho1 : nullptr,
-                                                                    e->u, e->D, d, e->N);
-    LBF_CK(e, cudaGetLastError());
+    const Grid g = grid_of(e);
+    const double* r1 = color ? e->rho1 : nullptr;
+    if (dst == Dest::kDevice) {
+        fields_range_kernel<<<dense_blocks(e->N), 256, 0, e->stream>>>(g, e->rho0, r1, e->u, e->D, 0, e->N, out);
+        LBF_CK(e, cudaGetLastError());
+        return LBF_OK;
+    }
+    double* st = nullptr;
+    if ((rc = stage_buffer(e, &st))) return rc;
+    const size_t chunk = kStageBytes / (sizeof(double) * per);
+    const size_t vec = (size_t)(1 + (color ? 1 : 0)) * e->N;   // offset of the velocity array in out
+    for (size_t v0 = 0; v0 < e->N; v0 += chunk) {
+        const size_t r = std::min(chunk, e->N - v0);
+        fields_range_kernel<<<dense_blocks(r), 256, 0, e->stream>>>(g, e->rho0, r1, e->u, e->D, v0, r, st);
+        LBF_CK(e, cudaGetLastError());
+        LBF_CK(e, cudaMemcpyAsync(out + v0, st, r * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+        if (color)
+            LBF_CK(e, cudaMemcpyAsync(out + e->N + v0, st + r, r * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+        LBF_CK(e, cudaMemcpyAsync(out + vec + (size_t)e->D * v0, st + (size_t)(1 + (color ? 1 : 0)) * r,
+                                  (size_t)e->D * r * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    }
     return LBF_OK;
 }
 
@@ -1139,8 +1223,9 @@ int lbf_populations_dense_async(lbf_engine* e, double* out, size_t n)
     if (n != blocks * e->N) return fail(e, LBF_EINVAL, "population buffer must hold phases*Q*N doubles");
     int rc = setdev(e);
     if (rc) return rc;
-    double* d = device_writable(e, out);
-    if (!d) return fail(e, LBF_EINVAL, "out must be device memory of the engine's device or page-locked host memory");
+    const Dest dst = destination(e, out);
+    if (dst == Dest::kNone)
+        return fail(e, LBF_EINVAL, "out must be device memory of the engine's device or page-locked host memory");
     const double* src = static_cast<const double*>(e->f[e->cur]);
     if (e->cfg.storage != LBF_STORE_FP64) {
         if (!e->dense_tmp && (rc = dalloc(e, &e->dense_tmp, blocks * e->nfp))) return rc;
@@ -1150,9 +1235,23 @@ int lbf_populations_dense_async(lbf_engine* e, double* out, size_t n)
         src = e->dense_tmp;
     }
     if (e->N == 0) return LBF_OK;
-    populations_dense_kernel<<<dense_blocks(e->N), 256, 0, e->stream>>>(grid_of(e), src, (int)blocks, d, e->N,
-                                                                        e->err);
-    LBF_CK(e, cudaGetLastError());
+    const Grid g = grid_of(e);
+    if (dst == Dest::kDevice) {
+        populations_range_kernel<<<dense_blocks(e->N), 256, 0, e->stream>>>(g, src, (int)blocks, 0, e->N, out, e->err);
+        LBF_CK(e, cudaGetLastError());
+        return LBF_OK;
+    }
+    double* st = nullptr;
+    if ((rc = stage_buffer(e, &st))) return rc;
+    const size_t chunk = kStageBytes / (sizeof(double) * blocks);
+    for (size_t v0 = 0; v0 < e->N; v0 += chunk) {
+        const size_t r = std::min(chunk, e->N - v0);
+        populations_range_kernel<<<dense_blocks(r), 256, 0, e->stream>>>(g, src, (int)blocks, v0, r, st, e->err);
+        LBF_CK(e, cudaGetLastError());
+        // [block][r] in the stage -> [block][N] at voxel v0 in out.
+        LBF_CK(e, cudaMemcpy2DAsync(out + v0, e->N * sizeof(double), st, r * sizeof(double), r * sizeof(double),
+                                    blocks, cudaMemcpyDeviceToHost, e->stream));
+    }
     return LBF_OK;
 }
 

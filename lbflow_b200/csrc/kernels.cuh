@@ -348,6 +348,7 @@ struct ScspParams {
     int mrt = 0;       // MRT: mass and momentum rows are not relaxed (rate 0)
     uint32_t seed = 0; // non-zero: stochastic rounding of 16-bit float storage (per-step seed)
     uint32_t node0 = 0; // first node of the geometry: rounding streams follow the geometry's own node order
+    int reverse = 0;    // blocks in descending node order (alternated every step; see scsp_step)
 };
 
 // Integer hash (lowbias32 of C. Wellons) seeding the per-node rounding stream.
@@ -450,7 +451,11 @@ scsp_step(const Grid g, const Force F, const ScspParams P,
           Macros mo, const int out, uint32_t* __restrict__ err,
           const int8_t* __restrict__ ein, int8_t* __restrict__ eout)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    // The node order alternates between steps: a step that runs in the
+    // opposite order to the previous one starts with the nodes whose
+    // populations that step wrote last, which are still in L2.
+    const uint32_t blk = P.reverse ? gridDim.x - 1 - blockIdx.x : blockIdx.x;
+    const uint32_t i = blk * blockDim.x + threadIdx.x;
     if (i >= g.nf) return;
     scsp_update<L, S, PULL>(g, F, P, fin, fout, i, mo, out, err, ein, eout);
 }

@@ -449,6 +449,36 @@ def warm_start(engine, net, fluid, tau, g, rho0=1.0, block=8, mode='darcy', velo
     return fields
 
 
+def block_mobility(s, g, b, rho0=1.0):
+    """Block mobility of a running state from its block sums s (d, h, w, 5) =
+    (sum rho, sum u_x, sum u_y, sum u_z, fluid voxels) over b^3 blocks: with
+    the block flux q = sum u / b^3, the block pressure phi = (rho_b - rho0) /
+    (3 rho0) and the driving force per unit mass g x_hat - grad phi (central
+    differences), the least-squares M of q = M (g x_hat - grad phi) over the
+    three components.  Returns (M, fluid voxels, phi); M is 0 where the drive
+    vanishes."""
+    cnt = s[..., 4]
+    rho_b = torch.where(cnt > 0, s[..., 0] / cnt.clamp(min=1.0), torch.full_like(cnt, rho0))
+    q = s[..., 1:4] / float(b ** 3)
+    phi = (rho_b - rho0) / (3.0 * rho0)
+    drive = []
+    for c, ax in enumerate(_AXES):
+        grad = (_shift(phi, -1, ax) - _shift(phi, 1, ax)) / (2.0 * b)
+        drive.append((g if c == 0 else 0.0) - grad)
+    num = sum(q[..., c] * drive[c] for c in range(3))
+    den = sum(d * d for d in drive)
+    mob = torch.where(den > 0, num / den.clamp(min=1e-300), torch.zeros_like(num))
+    return mob, cnt, phi
+
+
+def block_sums_dense(rho, u, fluid, b):
+    """block_sums of dense fields: rho (D, H, W), u (3, D, H, W) (zero on
+    solids), fluid (D, H, W) -> (D/b, H/b, W/b, 5) float64."""
+    m = fluid.double()
+    parts = [rho.double() * m, u[0].double(), u[1].double(), u[2].double(), m]
+    return torch.stack([_block_mean(x[..., None], b)[..., 0] * float(b ** 3) for x in parts], dim=-1)
+
+
 class DarcyAccelerator:
     """Block-scale pressure correction of a running single-phase engine.
 
@@ -507,17 +537,7 @@ class DarcyAccelerator:
         s = torch.empty(D // b, H // b, W // b, 5, dtype=torch.float64, device=dev)
         self.engine.block_sums(b, out=s)
         mark('block_sums')
-        cnt = s[..., 4]
-        rho_b = torch.where(cnt > 0, s[..., 0] / cnt.clamp(min=1.0), torch.full_like(cnt, rho0))
-        q = s[..., 1:4] / float(b ** 3)
-        phi = (rho_b - rho0) / (3.0 * rho0)
-        drive = []
-        for c, ax in enumerate(_AXES):
-            grad = (_shift(phi, -1, ax) - _shift(phi, 1, ax)) / (2.0 * b)
-            drive.append((g if c == 0 else 0.0) - grad)
-        num = sum(q[..., c] * drive[c] for c in range(3))
-        den = sum(d * d for d in drive)
-        mob = torch.where(den > 0, num / den.clamp(min=1e-300), torch.zeros_like(num))
+        mob, cnt, phi = block_mobility(s, g, b, rho0)
         mob = torch.clamp(mob, min=1e-3 * float(mob.clamp(min=0).mean()) + 1e-30)
         mark('mobility')
         if mob.is_cuda and self.face == 'geometric':
@@ -548,6 +568,177 @@ def load(path, device='cuda'):
     if tuple(ck['ch']) != CH:
         raise ValueError(f'weights are for channels {ck["ch"]}, this network has {CH}')
     net = WarmStartNet()
+    net.load_state_dict(ck['state'])
+    return net.to(device), ck.get('meta', {})
+
+
+# ------------------------------------------------------ learned mobility --
+# The block Darcy correction (DarcyAccelerator) has to wait a few hundred
+# steps of the run from rest before it can estimate each block's mobility
+# from the developed local flow.  The mobility of a block is a local,
+# geometry-only property (at fixed viscosity), so a convolutional network
+# can predict it from the voxels at t = 0; the upscaled Darcy problem (the
+# library's CUDA solve) then supplies the domain-scale coupling that a local
+# network cannot see, and the run starts with its block-scale pressure in
+# place.  Targets are the accelerator's own estimates after MOB_STEPS steps
+# from rest, the state it corrects from.
+
+MOB_BLOCK = 2
+MOB_STEPS = 500
+
+
+class MobilityNet(WarmStartNet):
+    """WarmStartNet whose head channel 0 is the log block mobility
+    log(M nu) (M of block_mobility, nu = (tau - 1/2)/3) of the MOB_BLOCK^3
+    block a voxel lies in, normalised by `norm` = (mean, std); the block
+    value is the mean over its voxels."""
+
+    def __init__(self, seed=0):
+        super().__init__(seed)
+        self.register_buffer('norm', torch.tensor([0.0, 1.0]))
+
+    def blocks(self, x, b=MOB_BLOCK):
+        """x: (B, D, H, W, 8) features -> (B, D/b, H/b, W/b) normalised log mobility (float32)."""
+        y = self(x)[..., 0].float()
+        B, D, H, W = y.shape
+        return y.reshape(B, D // b, b, H // b, b, W // b, b).mean(dim=(2, 4, 6))
+
+
+def mobility_targets(rho, u, fluid, tau, g, b=MOB_BLOCK, rho0=1.0):
+    """Training target of one medium from its state after MOB_STEPS steps:
+    log(M nu) per block and the block's fluid voxel count as its weight
+    (float32, (D/b, H/b, W/b) each), M clamped below as the accelerator
+    clamps it."""
+    s = block_sums_dense(rho, u, fluid, b)
+    mob, cnt, _ = block_mobility(s, g, b, rho0)
+    mob = torch.clamp(mob, min=1e-3 * float(mob.clamp(min=0).mean()) + 1e-30)
+    nu = (tau - 0.5) / 3.0
+    return torch.log(mob * nu).float(), cnt.float()
+
+
+def _augment_blocks(feat, targ, wt, gen, b=MOB_BLOCK):
+    """Periodic shifts by whole blocks, y/z mirrors and the y<->z swap (the
+    block mobility is a scalar, so these leave it unchanged)."""
+    dims = feat.shape[1:4]
+    sh = [int(torch.randint(0, d // b, (1,), generator=gen)) for d in dims]
+    feat = torch.roll(feat, [v * b for v in sh], dims=(1, 2, 3))
+    targ = torch.roll(targ, sh, dims=(1, 2, 3))
+    wt = torch.roll(wt, sh, dims=(1, 2, 3))
+    for ax in (1, 2):
+        if torch.rand(1, generator=gen).item() < 0.5:
+            feat, targ, wt = feat.flip(ax), targ.flip(ax), wt.flip(ax)
+    if dims[0] == dims[1] and torch.rand(1, generator=gen).item() < 0.5:
+        feat, targ, wt = feat.transpose(1, 2), targ.transpose(1, 2), wt.transpose(1, 2)
+    return feat.contiguous(), targ.contiguous(), wt.contiguous()
+
+
+def train_mobility(net, samples, iters=3000, lr=2e-3, batch_voxels=2 * 96 ** 3, seed=0, log=None):
+    """samples: list of (fluid (D,H,W) bool cuda, log-mobility target and
+    weight, both (D/b,H/b,W/b) float cuda).  Weighted mean-square error of
+    the normalised block log mobility, AdamW with a cosine schedule; every
+    convolution and gradient on the tensor-core kernels.  Returns the loss
+    history."""
+    dev = samples[0][0].device
+    w_all = torch.cat([w.reshape(-1) for _, _, w in samples]).double()
+    t_all = torch.cat([t.reshape(-1) for _, t, _ in samples]).double()
+    mu = float((w_all * t_all).sum() / w_all.sum())
+    sd = float(torch.sqrt((w_all * (t_all - mu) ** 2).sum() / w_all.sum()).clamp(min=1e-6))
+    net.norm.copy_(torch.tensor([mu, sd]))
+    by_shape = {}
+    for i, (fl, _, _) in enumerate(samples):
+        by_shape.setdefault(tuple(fl.shape), []).append(i)
+    shapes = sorted(by_shape)
+    feats = [features(fl.unsqueeze(0))[0] for fl, _, _ in samples]
+    opt = torch.optim.AdamW(net.parameters(), lr=lr, weight_decay=1e-4)
+    gen = torch.Generator().manual_seed(seed)
+    hist = []
+    t0 = time.perf_counter()
+    for it in range(iters):
+        for gparam in opt.param_groups:
+            gparam['lr'] = lr * 0.5 * (1 + math.cos(math.pi * it / iters))
+        shp = shapes[int(torch.randint(0, len(shapes), (1,), generator=gen))]
+        pool = by_shape[shp]
+        nb = max(1, min(len(pool), batch_voxels // int(np.prod(shp))))
+        pick = [pool[int(j)] for j in torch.randint(0, len(pool), (nb,), generator=gen)]
+        fb, tb, wb = [], [], []
+        for j in pick:
+            f, t, w = _augment_blocks(feats[j].unsqueeze(0), samples[j][1].unsqueeze(0),
+                                      samples[j][2].unsqueeze(0), gen)
+            fb.append(f)
+            tb.append(t)
+            wb.append(w)
+        fb, tb, wb = torch.cat(fb), (torch.cat(tb) - mu) / sd, torch.cat(wb)
+        y = net.blocks(fb)
+        loss = (((y - tb) ** 2) * wb).sum() / wb.sum()
+        opt.zero_grad(set_to_none=True)
+        loss.backward()
+        torch.nn.utils.clip_grad_norm_(net.parameters(), 1.0)
+        opt.step()
+        if it % 50 == 0 or it == iters - 1:
+            lv = float(loss.detach())
+            hist.append((it, lv, time.perf_counter() - t0))
+            if log:
+                log(f'iter {it} loss {lv:.4e} shape {shp} batch {nb} {time.perf_counter() - t0:.1f}s')
+    conv.check(dev)
+    return hist
+
+
+def predict_mobility(net, fluid, tau, b=MOB_BLOCK):
+    """Block mobilities M (D/b, H/b, W/b) float64 of a fluid mask for
+    relaxation time tau, from the network (blocks without fluid get 0)."""
+    with torch.no_grad():
+        y = net.blocks(features(fluid.unsqueeze(0)), b)[0].double()
+        nu = (tau - 0.5) / 3.0
+        mob = torch.exp(y * float(net.norm[1]) + float(net.norm[0])) / nu
+        cnt = _block_mean(fluid.double()[..., None], b)[..., 0]
+        return torch.where(cnt > 0, mob, torch.zeros_like(mob))
+
+
+def evaluate_mobility(net, samples, tau=1.0):
+    """Per medium: weighted RMS error and correlation of the predicted log
+    block mobility against the target."""
+    out = []
+    for fl, t, w in samples:
+        p = torch.log((predict_mobility(net, fl, tau) * ((tau - 0.5) / 3.0)).clamp(min=1e-300)).float()
+        m = w > 0
+        d = (p - t)[m]
+        ww = w[m]
+        rms = float(torch.sqrt((ww * d * d).sum() / ww.sum()))
+        pc, tc = p[m] - (ww * p[m]).sum() / ww.sum(), t[m] - (ww * t[m]).sum() / ww.sum()
+        corr = float((ww * pc * tc).sum() / torch.sqrt((ww * pc * pc).sum() * (ww * tc * tc).sum()).clamp(min=1e-30))
+        out.append(dict(log_mob_rms=rms, log_mob_corr=corr))
+    return out
+
+
+def mobility_start(engine, net, fluid, tau, g, rho0=1.0, block=MOB_BLOCK, rtol=1e-3):
+    """Start `engine` (single phase, force g along +x) with the block Darcy
+    pressure of the predicted block mobilities: the same upscaled problem
+    and density change as DarcyAccelerator, applied at t = 0 to the rest
+    state, velocity at rest.  Returns the CG iterations of the solve."""
+    mob = predict_mobility(net, fluid, tau, block)
+    porous = mob > 0
+    mob = torch.clamp(mob, min=1e-3 * float(mob.clamp(min=0).mean()) + 1e-30)
+    target, it = darcy_pressure_device(mob, g, block, rtol=rtol)
+    m = fluid.double()
+    drho = 3.0 * rho0 * _upsample_periodic(target * porous, block) * m
+    drho = drho - drho.sum() / m.sum().clamp(min=1.0) * m
+    fields = torch.zeros(*fluid.shape, 4, dtype=torch.float32, device=fluid.device)
+    fields[..., 3] = (rho0 + drho).float()
+    torch.cuda.current_stream(fluid.device).synchronize()
+    engine.initialize_equilibrium(fields.contiguous())
+    return it
+
+
+def save_mobility(net, path, meta=None):
+    torch.save({'state': {k: v.detach().cpu() for k, v in net.state_dict().items()}, 'ch': CH,
+                'kind': 'mobility', 'meta': meta or {}}, path)
+
+
+def load_mobility(path, device='cuda'):
+    ck = torch.load(path, map_location='cpu', weights_only=False)
+    if tuple(ck['ch']) != CH or ck.get('kind') != 'mobility':
+        raise ValueError(f'{path} does not hold block-mobility weights for channels {CH}')
+    net = MobilityNet()
     net.load_state_dict(ck['state'])
     return net.to(device), ck.get('meta', {})
 

@@ -232,3 +232,58 @@ def test_multigrid_transfers_are_adjoint_and_solver_converges():
     rhs = 1e-5 * (mf[0] - torch.roll(mf[0], 1, 2)) / 2
     res = ws._apply(phi, mf, 2.0) - (rhs - rhs.mean())
     assert float(res.norm() / rhs.norm()) < 1e-7
+
+
+def test_block_mobility_of_uniform_and_pressure_driven_flow():
+    """The accelerator's estimator: M = q / (g - dphi/dx) along x, exact for
+    a uniform flux under a linear pressure ramp (periodic wrap excluded)."""
+    from lbflow_b200 import warmstart as ws
+    b, g = 2, 1e-5
+    nb = (3, 4, 6)
+    s = torch.zeros(*nb, 5, dtype=torch.float64)
+    s[..., 4] = b ** 3
+    s[..., 0] = b ** 3                       # rho = 1: no pressure gradient
+    s[..., 1] = 2.5e-6 * b ** 3               # q_x = 2.5e-6
+    mob, cnt, phi = ws.block_mobility(s, g, b)
+    assert torch.allclose(mob, torch.full(nb, 2.5e-6 / g, dtype=torch.float64))
+    assert torch.equal(cnt, s[..., 4]) and torch.all(phi == 0)
+    # Pressure rising along x by dp per block: drive = g - dp / b.
+    dp = 3e-6
+    x = torch.arange(nb[2], dtype=torch.float64)
+    rho = 1.0 + 3.0 * dp * x
+    s[..., 0] = rho * b ** 3
+    mob, _, _ = ws.block_mobility(s, g, b)
+    inner = mob[..., 1:-1]
+    assert torch.allclose(inner, torch.full_like(inner, 2.5e-6 / (g - dp / b)))
+
+
+def test_block_sums_dense_layout():
+    from lbflow_b200 import warmstart as ws
+    rng = np.random.default_rng(1)
+    fl = torch.from_numpy(rng.random((4, 6, 8)) < 0.5)
+    rho = torch.from_numpy(1 + rng.random((4, 6, 8)) * 1e-3) * fl
+    u = torch.from_numpy(rng.standard_normal((3, 4, 6, 8))) * fl
+    s = ws.block_sums_dense(rho, u, fl, 2)
+    assert s.shape == (2, 3, 4, 5)
+    blk = (slice(2, 4), slice(0, 2), slice(4, 6))
+    assert torch.isclose(s[1, 0, 2, 0], rho[blk].sum())
+    assert torch.isclose(s[1, 0, 2, 2], u[1][blk].sum())
+    assert s[1, 0, 2, 4] == fl[blk].sum()
+
+
+def test_mobility_network_shape_and_targets():
+    from lbflow_b200 import warmstart as ws
+    net = ws.MobilityNet()
+    assert net.norm.tolist() == [0.0, 1.0]
+    assert set(net.state_dict()) == set(ws.WarmStartNet().state_dict()) | {'norm'}
+    rng = np.random.default_rng(2)
+    fl = torch.from_numpy(rng.random((4, 4, 4)) < 0.6)
+    u = torch.zeros(3, 4, 4, 4, dtype=torch.float64)
+    u[0] = 1e-6 * fl
+    t, w = ws.mobility_targets(torch.ones(4, 4, 4, dtype=torch.float64) * fl, u, fl, 1.0, 1e-5)
+    assert t.shape == (2, 2, 2) and w.shape == (2, 2, 2)
+    # Blocks with fluid: q = 1e-6 * count / 8, M = q / g, target log(M nu).
+    for idx in np.ndindex(2, 2, 2):
+        if w[idx] > 0:
+            want = math.log(1e-6 * float(w[idx]) / 8 / 1e-5 / 6)
+            assert abs(float(t[idx]) - want) < 1e-5
