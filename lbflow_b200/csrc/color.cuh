@@ -8,6 +8,7 @@
 //           geometric wall rotation), perturbation and recoloring.
 // Solid voxels read as phi = 86 (SOLID_DENS_N, colorfluid.cpp:49).
 #pragma once
+#include <type_traits>
 #include "kernels.cuh"
 
 namespace lbf {
@@ -20,7 +21,70 @@ struct ColorParams {
     Trt rate;              // the uniform rates (used when uniform_tau)
     double ak;             // 2.25 sigma (colorfluid.cpp:305)
     double beta;           // recoloring parameter
+    uint32_t seed;         // 16-bit storage: per-step seed of the stochastic rounding (0: round to nearest)
 };
+
+// ---- 16-bit storage of the two components ---------------------------------------
+// The two components are kept as the total fT_q = f0_q + f1_q and the share
+// r_q = f0_q / fT_q of component 0:
+//   block 0: (fT_q - w_q rho0) * 4096 / w_q in IEEE half or bfloat16 -- the
+//            single-phase shifted form, so the velocity-carrying deviations
+//            keep their precision;
+//   block 1: r_q as 16-bit fixed point over [-0.5, 1.5) (resolution 2^-15),
+//            (recoloring keeps r_q within rho0/rho +- beta/4 of the node's
+//            phase share).
+// f0 = r fT, f1 = fT - f0, so the two components always add up to the stored
+// total.  Both are rounded stochastically when a seed is given (unbiased
+// stored values, as for single-phase 16-bit storage).  Arithmetic in FP32.
+template <class L, class H> struct ColorPacked {
+    static constexpr bool packed = true;
+    static constexpr bool blocked = false;
+    static constexpr bool dither = true;
+    static constexpr bool shifted = false;
+    using T = uint16_t;
+    using R = float;
+    static constexpr int kDrop = sizeof(H) == 2 && std::is_same<H, __half>::value ? 13 : 16;
+    __device__ static float to_f(uint16_t h)
+    {
+        if constexpr (std::is_same<H, __half>::value) return __half2float(__ushort_as_half(h));
+        else return __bfloat162float(__ushort_as_bfloat16(h));
+    }
+    __device__ static uint16_t from_f_rn(float x)
+    {
+        if constexpr (std::is_same<H, __half>::value) return __half_as_ushort(__float2half_rn(x));
+        else return __bfloat16_as_ushort(__float2bfloat16_rn(x));
+    }
+    __device__ static uint16_t from_f_sr(float x, uint32_t r)
+    {
+        if constexpr (std::is_same<H, __half>::value)
+            return __half_as_ushort(fabsf(x) >= 6.103515625e-05f ? __float2half_rz(dither_bits(x, r, 13))
+                                                                 : __float2half_rn(x));
+        else return __bfloat16_as_ushort(__float2bfloat16_rz(dither_bits(x, r, 16)));
+    }
+    __device__ static void load_pair(const uint16_t* __restrict__ fin, uint32_t off, uint32_t nblk, int q,
+                                     float rho_bar, float& f0, float& f1)
+    {
+        const float g = to_f(__ldg(fin + off)) * ShiftScale<L>::inv(q);
+        const float fT = (float)L::w36f(q) * (1.0f / 36.0f) * rho_bar + g;
+        const float r = (float)__ldg(fin + nblk + off) * (1.0f / 32768.0f) - 0.5f;
+        f0 = r * fT;
+        f1 = fT - f0;
+    }
+    // a0 = component 0, fT = the total; r1, r2 random words (unused when !sr).
+    __device__ static void store_pair(uint16_t* __restrict__ fout, uint32_t off, uint32_t nblk, int q,
+                                      float rho_bar, float a0, float fT, bool sr, uint32_t r1, uint32_t r2)
+    {
+        const float g = (fT - (float)L::w36f(q) * (1.0f / 36.0f) * rho_bar) * ShiftScale<L>::scale(q);
+        fout[off] = sr ? from_f_sr(g, r1) : from_f_rn(g);
+        const float share = fabsf(fT) > 1e-30f ? a0 / fT : 0.5f;
+        float c = (share + 0.5f) * 32768.0f + (sr ? (float)(r2 >> 8) * (1.0f / 16777216.0f) : 0.5f);
+        c = fminf(fmaxf(c, 0.0f), 65535.0f);
+        fout[nblk + off] = (uint16_t)c;
+    }
+};
+
+template <class S> struct IsPacked { static constexpr bool value = false; };
+template <class L, class H> struct IsPacked<ColorPacked<L, H>> { static constexpr bool value = true; };
 
 struct ColorWall {
     const uint16_t* __restrict__ angle_id;  // per fluid node; 0 = not next to a solid
@@ -59,20 +123,24 @@ __device__ __forceinline__ uint32_t film_sources(const Grid& g, const uint32_t* 
 template <class L, class S, bool PULL, bool FILM>
 __device__ __forceinline__ void color_gather(const Grid& g, const Film& film, const typename S::T* __restrict__ fin,
                                              uint32_t i, int x, int y, int z, typename S::R (&f0)[L::Q],
-                                             typename S::R (&f1)[L::Q], uint32_t (&nbr)[L::Q])
+                                             typename S::R (&f1)[L::Q], uint32_t (&nbr)[L::Q],
+                                             typename S::R rho_bar = typename S::R(0))
 {
     using R = typename S::R;
     // One neighbour lookup for both components (the sources are the same).
     const typename S::T* __restrict__ fin1 = fin + (size_t)L::Q * g.nfp;
     const uint32_t nfp = g.nfp;
-    f0[0] = S::load(fin + i, 0, R(0));
-    f1[0] = S::load(fin1 + i, 0, R(0));
+    const uint32_t nblk = (uint32_t)L::Q * nfp;
+    auto load2 = [&](uint32_t off, int q, R& a, R& b) {
+        if constexpr (IsPacked<S>::value) S::load_pair(fin, off, nblk, q, rho_bar, a, b);
+        else { a = S::load(fin + off, q, R(0)); b = S::load(fin1 + off, q, R(0)); }
+    };
+    load2(i, 0, f0[0], f1[0]);
     nbr[0] = i;
     if constexpr (!PULL) {
 #pragma unroll
         for (int q = 1; q < L::Q; ++q) {
-            f0[q] = S::load(fin + (q * nfp + i), q, R(0));
-            f1[q] = S::load(fin1 + (q * nfp + i), q, R(0));
+            load2(q * nfp + i, q, f0[q], f1[q]);
             nbr[q] = 0;
         }
     } else {
@@ -84,11 +152,10 @@ __device__ __forceinline__ void color_gather(const Grid& g, const Film& film, co
             const uint32_t node = fluid ? src[q] : i;
             nbr[L::op(q)] = fluid ? src[q] : 0xffffffffu;
             const uint32_t off = (fluid ? (uint32_t)q : (uint32_t)L::op(q)) * nfp + node;
-            f0[q] = S::load(fin + off, q, R(0));
-            f1[q] = S::load(fin1 + off, q, R(0));
+            load2(off, q, f0[q], f1[q]);
         }
     }
-    if constexpr (FILM && PULL) {
+    if constexpr (FILM && PULL && !IsPacked<S>::value) {
         const uint32_t b1 = film_sources<L>(g, film.bits[1], x, y, z);   // blocks phase 0
         const uint32_t b0 = film_sources<L>(g, film.bits[0], x, y, z);   // blocks phase 1
         const typename S::T* in1 = fin + (size_t)L::Q * g.nfp;
@@ -129,7 +196,7 @@ template <class L> constexpr int normal_codes() { return L::D == 3 ? 11 * 11 * 1
 template <class L, class S, bool PULL, bool FILM>
 __global__ void __launch_bounds__(128)
 color_phase(const Grid g, const Film film, const typename S::T* __restrict__ fin, double* __restrict__ phi,
-            uint32_t* __restrict__ err)
+            uint32_t* __restrict__ err, const double rho_bar)
 {
     using R = typename S::R;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -138,7 +205,7 @@ color_phase(const Grid g, const Film film, const typename S::T* __restrict__ fin
     unpack(__ldg(&g.coord[i]), x, y, z);
     R f0[L::Q], f1[L::Q];
     uint32_t nbr[L::Q];
-    color_gather<L, S, PULL, FILM>(g, film, fin, i, x, y, z, f0, f1, nbr);
+    color_gather<L, S, PULL, FILM>(g, film, fin, i, x, y, z, f0, f1, nbr, R(rho_bar));
     R d0 = f0[0], d1 = f1[0];
 #pragma unroll
     for (int q = 1; q < L::Q; ++q) { d0 += f0[q]; d1 += f1[q]; }
@@ -335,6 +402,22 @@ __device__ __forceinline__ void color_update(const Grid& g, const Force& F, cons
     const R dens0T = d0 / dt;
     typename S::T* o0 = fout;
     typename S::T* o1 = fout + (size_t)L::Q * g.nfp;
+    // 16-bit storage: one linear congruential stream per node and step.
+    uint32_t rng = IsPacked<S>::value && P.seed ? hash32(i * 0x9e3779b9u + P.seed) : 0u;
+    auto put = [&](int q, R a0, R tot) {
+        if constexpr (IsPacked<S>::value) {
+            uint32_t r1 = 0, r2 = 0;
+            if (P.seed) {
+                rng = rng * 1664525u + 1013904223u; r1 = rng;
+                rng = rng * 1664525u + 1013904223u; r2 = rng;
+            }
+            S::store_pair(fout, (uint32_t)q * g.nfp + i, (uint32_t)L::Q * g.nfp, q, R(P.rho_ref[0]), a0, tot,
+                          P.seed != 0, r1, r2);
+        } else {
+            S::store(o0 + (size_t)q * g.nfp + i, a0, q, R(0));
+            S::store(o1 + (size_t)q * g.nfp + i, tot - a0, q, R(0));
+        }
+    };
     if (norm > R(1e-9)) {
         const R betaDens01TT = R(P.beta) * dens0T * d1 / dt;
         const R AkNorm = R(P.ak) * norm / tau;
@@ -351,16 +434,11 @@ __device__ __forceinline__ void color_update(const Grid& g, const Force& F, cons
             fT[q] += AkNorm * (R(w<L>(q)) * angle * angle - R(L::B(q)));
             if (q != 0 && !axis_dir<L>(q)) angle /= R(1.4142135623730951);
             const R a0 = dens0T * fT[q] + betaDens01TT * angle * fu0[q];
-            S::store(o0 + (size_t)q * g.nfp + i, a0, q, R(0));
-            S::store(o1 + (size_t)q * g.nfp + i, fT[q] - a0, q, R(0));
+            put(q, a0, fT[q]);
         }
     } else {
 #pragma unroll
-        for (int q = 0; q < L::Q; ++q) {
-            const R a0 = dens0T * fT[q];
-            S::store(o0 + (size_t)q * g.nfp + i, a0, q, R(0));
-            S::store(o1 + (size_t)q * g.nfp + i, fT[q] - a0, q, R(0));
-        }
+        for (int q = 0; q < L::Q; ++q) put(q, dens0T * fT[q], fT[q]);
     }
 }
 
@@ -386,7 +464,7 @@ color_collide(const Grid g, const Film film, const Force F, const ColorParams P,
     unpack(__ldg(&g.coord[i]), x, y, z);
     R f0[L::Q], f1[L::Q];
     uint32_t nbr[L::Q];
-    color_gather<L, S, PULL, FILM>(g, film, fin, i, x, y, z, f0, f1, nbr);
+    color_gather<L, S, PULL, FILM>(g, film, fin, i, x, y, z, f0, f1, nbr, R(P.rho_ref[0]));
     if (!PULL) {
         // t = 0: neighbours by direct lookup (the pull above read local values).
 #pragma unroll
@@ -469,14 +547,14 @@ __device__ __forceinline__ void color_zou_he_gather(const Grid& g, const Film& f
                                                     const typename S::T* __restrict__ fin, uint32_t& i,
                                                     typename S::R (&f0)[L::Q], typename S::R (&f1)[L::Q],
                                                     uint32_t (&nbr)[L::Q], typename S::R& dens,
-                                                    typename S::R& ua, int& axis)
+                                                    typename S::R& ua, int& axis, typename S::R rho_bar)
 {
     i = __ldg(&z.node[k]);
     const uint32_t code = __ldg(&z.code[k]);
     const double val = __ldg(&z.value[k]);
     int x, y, zc;
     unpack(__ldg(&g.coord[i]), x, y, zc);
-    color_gather<L, S, true, FILM>(g, film, fin, i, x, y, zc, f0, f1, nbr);
+    color_gather<L, S, true, FILM>(g, film, fin, i, x, y, zc, f0, f1, nbr, rho_bar);
     const uint32_t kind = (code >> 8) & 0xffu;
     const int phs = (int)(code >> 16);
     const int dir = (int)(code & 0xffu);
@@ -499,7 +577,7 @@ __device__ __forceinline__ void color_zou_he_gather(const Grid& g, const Film& f
 template <class L, class S, bool FILM>
 __global__ void __launch_bounds__(128)
 color_zou_he_phase(const Grid g, const Film film, const ZouHe z, const typename S::T* __restrict__ fin,
-                   double* __restrict__ phi, uint32_t* __restrict__ err)
+                   double* __restrict__ phi, uint32_t* __restrict__ err, const double rho_bar)
 {
     using R = typename S::R;
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -508,7 +586,7 @@ color_zou_he_phase(const Grid g, const Film film, const ZouHe z, const typename 
     R f0[L::Q], f1[L::Q], dens, ua;
     uint32_t nbr[L::Q];
     int axis;
-    color_zou_he_gather<L, S, FILM>(g, film, z, k, fin, i, f0, f1, nbr, dens, ua, axis);
+    color_zou_he_gather<L, S, FILM>(g, film, z, k, fin, i, f0, f1, nbr, dens, ua, axis, R(rho_bar));
     R d0 = f0[0], d1 = f1[0];
 #pragma unroll
     for (int q = 1; q < L::Q; ++q) { d0 += f0[q]; d1 += f1[q]; }
@@ -536,7 +614,7 @@ color_zou_he_collide(const Grid g, const Film film, const Force F, const ColorPa
     R f0[L::Q], f1[L::Q], dens, ua;
     uint32_t nbr[L::Q];
     int axis;
-    color_zou_he_gather<L, S, FILM>(g, film, z, k, fin, i, f0, f1, nbr, dens, ua, axis);
+    color_zou_he_gather<L, S, FILM>(g, film, z, k, fin, i, f0, f1, nbr, dens, ua, axis, R(P.rho_ref[0]));
     R d0 = f0[0], d1 = f1[0];
 #pragma unroll
     for (int q = 1; q < L::Q; ++q) { d0 += f0[q]; d1 += f1[q]; }
@@ -554,18 +632,26 @@ color_zou_he_collide(const Grid g, const Film film, const Force F, const ColorPa
 // reference's initial calcMacroVar covers PB/VB).
 template <class L, class S>
 __global__ void __launch_bounds__(128)
-color_zou_he_record(const Grid g, const ZouHe z, const typename S::T* __restrict__ fin)
+color_zou_he_record(const Grid g, const ZouHe z, const typename S::T* __restrict__ fin, const double rho_bar)
 {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= z.n) return;
     const uint32_t i = __ldg(&z.node[k]);
     double d0 = 0.0, d1 = 0.0;
     {
-        typename S::R a = S::load(fin + i, 0, typename S::R(0)), b = S::load(fin + (size_t)L::Q * g.nfp + i, 0, typename S::R(0));
+        using R = typename S::R;
+        R a = R(0), b = R(0);
 #pragma unroll
-        for (int q = 1; q < L::Q; ++q) {
-            a += S::load(fin + (size_t)q * g.nfp + i, q, typename S::R(0));
-            b += S::load(fin + ((size_t)L::Q + q) * g.nfp + i, q, typename S::R(0));
+        for (int q = 0; q < L::Q; ++q) {
+            R p0, p1;
+            if constexpr (IsPacked<S>::value)
+                S::load_pair(fin, (uint32_t)q * g.nfp + i, (uint32_t)L::Q * g.nfp, q, R(rho_bar), p0, p1);
+            else {
+                p0 = S::load(fin + (size_t)q * g.nfp + i, q, R(0));
+                p1 = S::load(fin + ((size_t)L::Q + q) * g.nfp + i, q, R(0));
+            }
+            a = q == 0 ? p0 : a + p0;
+            b = q == 0 ? p1 : b + p1;
         }
         d0 = (double)a;
         d1 = (double)b;
@@ -594,8 +680,13 @@ __global__ void color_init(const Grid g, const Force F, const ColorParams P,
         ef += L::ex(q) * Fv[0];
         double v = P.ai[ph][q] * P.rho_ref[ph];
         v -= 1.5 * (L::w36f(q) / 36.0) * ef;
-        S::store(f + ((size_t)ph * L::Q + q) * g.nfp + i, R(v), q, R(0));
-        S::store(f + ((size_t)(1 - ph) * L::Q + q) * g.nfp + i, R(0), q, R(0));
+        if constexpr (IsPacked<S>::value) {
+            S::store_pair(f, (uint32_t)q * g.nfp + i, (uint32_t)L::Q * g.nfp, q, R(P.rho_ref[0]),
+                          ph == 0 ? R(v) : R(0), R(v), false, 0u, 0u);
+        } else {
+            S::store(f + ((size_t)ph * L::Q + q) * g.nfp + i, R(v), q, R(0));
+            S::store(f + ((size_t)(1 - ph) * L::Q + q) * g.nfp + i, R(0), q, R(0));
+        }
     }
 }
 

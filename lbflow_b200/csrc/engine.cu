@@ -230,6 +230,10 @@ void launch_step(lbf_engine* e, bool pull, int out)
         // main kernel reproduces from their initial populations.
         if (pull && e->zh.n) launch_scsp_zou_he(e->D, (int)e->cfg.storage, a, e->zh);
     } else {
+        // 16-bit storage rounds stochastically with a fresh seed every pull
+        // step, as the single-phase path does.
+        const bool dither = e->cfg.storage == LBF_STORE_FP16 || e->cfg.storage == LBF_STORE_BF16;
+        e->cp.seed = dither && pull ? (++e->steps * 2654435761u) | 1u : 0u;
         ColorWall W{e->angle_id, e->angles, e->tib};
         ColorLaunch a{grid_of(e), e->force, e->cp, W, fin, fout, e->phi, macros_of(e), e->err, e->stream, e->zh,
                       Film{{e->film_bits[0], e->film_bits[1]}}};
@@ -323,6 +327,36 @@ __global__ void compress_blk_kernel(const double* __restrict__ in, int16_t* __re
     ex[i] = (int8_t)e;
 }
 
+// Two-phase 16-bit storage (total + component-0 share) <-> FP64 components.
+template <class L, class S>
+__global__ void expand_packed_kernel(const uint16_t* __restrict__ in, double* __restrict__ out, uint32_t nf,
+                                     uint32_t nfp, float rho_bar)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nf) return;
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) {
+        float f0, f1;
+        S::load_pair(in, (uint32_t)q * nfp + i, (uint32_t)L::Q * nfp, q, rho_bar, f0, f1);
+        out[(size_t)q * nfp + i] = (double)f0;
+        out[((size_t)L::Q + q) * nfp + i] = (double)f1;
+    }
+}
+
+template <class L, class S>
+__global__ void compress_packed_kernel(const double* __restrict__ in, uint16_t* __restrict__ out, uint32_t nf,
+                                       uint32_t nfp, float rho_bar)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nf) return;
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) {
+        const double a = in[(size_t)q * nfp + i], b = in[((size_t)L::Q + q) * nfp + i];
+        S::store_pair(out, (uint32_t)q * nfp + i, (uint32_t)L::Q * nfp, q, rho_bar, (float)a, (float)(a + b), false,
+                      0u, 0u);
+    }
+}
+
 template <class L>
 void convert(const lbf_engine* e, bool expand, void* f, double* tmp)
 {
@@ -343,7 +377,19 @@ void convert(const lbf_engine* e, bool expand, void* f, double* tmp)
         if (expand) expand_kernel<L, S><<<b, t, 0, e->stream>>>((const T*)f, tmp, e->nf, e->nfp, e->phases, r0); \
         else compress_kernel<L, S><<<b, t, 0, e->stream>>>(tmp, (T*)f, e->nf, e->nfp, e->phases, r0); \
     } while (0)
-    if (e->cfg.model == LBF_MODEL_COLOR) LBF_CONV(StoreF32Full, float);
+    if (e->cfg.model == LBF_MODEL_COLOR && (e->cfg.storage == LBF_STORE_FP16 || e->cfg.storage == LBF_STORE_BF16)) {
+        const float rb = (float)e->cp.rho_ref[0];
+#define LBF_PACKED(H)                                                                          \
+        do {                                                                                   \
+            using S = ColorPacked<L, H>;                                                       \
+            if (expand) expand_packed_kernel<L, S><<<b, t, 0, e->stream>>>((const uint16_t*)f, tmp, e->nf, e->nfp, rb); \
+            else compress_packed_kernel<L, S><<<b, t, 0, e->stream>>>(tmp, (uint16_t*)f, e->nf, e->nfp, rb); \
+        } while (0)
+        if (e->cfg.storage == LBF_STORE_FP16) LBF_PACKED(__half);
+        else LBF_PACKED(__nv_bfloat16);
+#undef LBF_PACKED
+    }
+    else if (e->cfg.model == LBF_MODEL_COLOR) LBF_CONV(StoreF32Full, float);
     else if (e->cfg.storage == LBF_STORE_FP16) LBF_CONV(StoreF16<L>, __half);
     else if (e->cfg.storage == LBF_STORE_BF16) LBF_CONV(StoreBF16<L>, __nv_bfloat16);
     else LBF_CONV(StoreF32<L>, float);
@@ -627,9 +673,8 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
     if (c.collision != LBF_SRT && c.collision != LBF_MRT)
         return fail(nullptr, LBF_EINVAL, "unknown collision model");
     if (c.storage > LBF_STORE_BFP16) return fail(nullptr, LBF_EINVAL, "unknown storage");
-    if (c.model == LBF_MODEL_COLOR && (c.storage == LBF_STORE_FP16 || c.storage == LBF_STORE_BF16 ||
-                                       c.storage == LBF_STORE_BFP16))
-        return fail(nullptr, LBF_EINVAL, "two-phase storage must be FP64 or FP32");
+    if (c.model == LBF_MODEL_COLOR && c.storage == LBF_STORE_BFP16)
+        return fail(nullptr, LBF_EINVAL, "two-phase storage must be FP64, FP32, FP16 or BF16");
     const int phases = c.model == LBF_MODEL_COLOR ? 2 : 1;
     for (int k = 0; k < phases; ++k)
         if (!std::isfinite(c.tau[k]) || c.tau[k] <= 0.5 || !std::isfinite(c.rho[k]) || c.rho[k] <= 0.0)
@@ -811,6 +856,8 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
     // Half-film bitmaps in the occupancy word layout (simulator.cpp:418-421).
     bool films = false;
     for (int l = 0; l < 256; ++l) films |= used[l] && labels[l].type == LBF_HF;
+    if (films && (c.storage == LBF_STORE_FP16 || c.storage == LBF_STORE_BF16))
+        return bail(LBF_EINVAL, "half-permeable films (HF) need FP64 or FP32 storage");
     if (films) {
         std::vector<uint32_t> fb[2] = {std::vector<uint32_t>(rows * e->W, 0u), std::vector<uint32_t>(rows * e->W, 0u)};
         for (size_t v = 0; v < e->N; ++v) {

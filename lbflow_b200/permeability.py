@@ -22,15 +22,16 @@ def permeability(engine, tau, g, axis=0):
 
 
 def converge(engine, tau, g, report=1000, tol=1e-6, max_steps=2_000_000, initialized=False,
-             on_report=None, warm=None, patience=5, t0=None, accelerate=None):
+             on_report=None, warm=None, patience=5, t0=None, accelerate=None, stall_floor=None):
     """Step to the reference's convergence criterion; returns a dict with the
     completed steps, wall seconds (device work included), K and the residual history.
 
     warm: optional callable that initialises the engine (a warm start).  The
     run then falls back to LBFlow's start from rest (engine.initialize) when
     the warm-started residual is non-finite, the device reports a numerical
-    error, or the residual, still above 100 * tol, sets no new minimum for
-    `patience` reports.  Steps
+    error, or the residual, still above `stall_floor` (default 100 * tol;
+    16-bit storage needs a higher one, as its rounding noise keeps the
+    residual near 1e-4), sets no new minimum for `patience` reports.  Steps
     and seconds count both attempts; `fallback` in the result says whether it
     happened.  t0: perf_counter value the seconds count from (default: the
     start of this call, after the engine's queued work).  accelerate:
@@ -102,7 +103,7 @@ def converge(engine, tau, g, report=1000, tol=1e-6, max_steps=2_000_000, initial
         # A stall far above the tolerance means the warm start went wrong; near
         # the tolerance it is the storage precision's floor, which a restart
         # would not change.
-        if warm_active and since_best >= patience and best > 100 * tol:
+        if warm_active and since_best >= patience and best > (stall_floor if stall_floor else 100 * tol):
             restart()
     engine.synchronize()
     seconds = time.perf_counter() - t0

@@ -54,7 +54,7 @@ def _create(**over):
     (dict(labels={0: ('VB', float('nan'), 1, 0)}), 'Non-finite boundary value'),
     (dict(labels={0: ('GV', 1e-6, 19, 0)}), 'body-force direction'),
     (dict(labels={0: ('VD', 0, 0, 1)}), 'phase'),
-    (dict(model=1, storage=1), 'two-phase storage'),
+    (dict(model=1, storage=4), 'two-phase storage'),
 ])
 def test_create_rejects_invalid_input(over, msg):
     rc, err = _create(**over)

@@ -117,3 +117,53 @@ def test_color_fp32_storage_tracks_fp64(steps):
     du = np.abs(out['fp32'][3] - out['fp64'][3]).max() / max(np.abs(out['fp64'][3]).max(), 1e-30)
     print(f'steps {steps}: phase-0 mass rel diff {abs(m32 - m64) / m64:.2e}, max |du|/max|u| {du:.2e}')
     assert du < 1e-2
+
+
+# Bounds of the two-phase quantities after 2,000 steps on the two-phase
+# workload's recipe (relative to FP64): phase-0 saturation, change of the
+# phase-0 mass over the run, phase-fraction-weighted Darcy flux of each phase
+# along the force (porous_media.py:33-41).
+COLOR_BOUNDS = {
+    'fp32': dict(saturation=1e-5, mass_drift=1e-5, flux=1e-3),
+    'fp16': dict(saturation=2e-3, mass_drift=2e-3, flux=5e-2),
+    'bf16': dict(saturation=1e-2, mass_drift=1e-2, flux=2e-1),
+}
+
+
+@pytest.fixture(scope='module')
+def color_fp64():
+    return _color_run('fp64')
+
+
+def _color_run(storage, steps=2000):
+    from lbflow_b200 import Engine
+    g, labels = _color_porous(n=(96, 48, 48), seed=8)
+    with Engine(g, labels, model='color', collision='MRT', tau=(1.0, 0.7), rho=(1.0, 1.0), alpha0=1 / 3,
+                sigma=1e-3, beta=0.7, storage=storage) as e:
+        e.initialize()
+        s0 = e.flux_sums()
+        e.step(steps, macros=True)
+        e.check()
+        s1 = e.flux_sums()
+        nf = e.fluid_nodes
+    return dict(saturation=s1[8] / nf, mass0=s0[6], mass1=s1[6], flux0=s1[5], flux1=s1[2] - s1[5])
+
+
+@pytest.mark.parametrize('storage', ['fp32', 'fp16', 'bf16'])
+def test_color_reduced_storage_phase_measures(color_fp64, storage):
+    """FP32 populations, and the 16-bit total + component-share storage,
+    against FP64 on a crop of the two-phase workload's recipe: saturation,
+    phase-0 mass drift and both phases' weighted Darcy fluxes."""
+    ref = color_fp64
+    got = _color_run(storage)
+    b = COLOR_BOUNDS[storage]
+    e_sat = abs(got['saturation'] - ref['saturation']) / ref['saturation']
+    drift = (got['mass1'] - got['mass0']) / got['mass0']
+    drift64 = (ref['mass1'] - ref['mass0']) / ref['mass0']
+    e_f0 = abs(got['flux0'] - ref['flux0']) / abs(ref['flux0'])
+    e_f1 = abs(got['flux1'] - ref['flux1']) / abs(ref['flux1'])
+    print(f'{storage}: saturation {e_sat:.2e}, phase-0 mass drift {drift:.2e} (fp64 {drift64:.2e}), '
+          f'phase flux errors {e_f0:.2e} / {e_f1:.2e}')
+    assert e_sat < b['saturation']
+    assert abs(drift - drift64) < b['mass_drift']
+    assert e_f0 < b['flux'] and e_f1 < b['flux']

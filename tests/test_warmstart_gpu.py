@@ -260,6 +260,40 @@ def test_trained_operator_starts_closer_to_the_steady_state():
     assert abs(runs['warm']['K'] - K) <= 1e-4 * abs(K) and not runs['warm']['fallback']
 
 
+MOB_WEIGHTS = WEIGHTS.parent / 'mobility.pt'
+
+
+@pytest.mark.skipif(not MOB_WEIGHTS.exists(), reason='trained block-mobility weights not present')
+def test_learned_mobility_start_reaches_the_band_sooner_than_rest():
+    """The learned start (block mobilities from the trained network, the
+    block Darcy pressure at t = 0) on a medium of the cube recipe that no
+    training medium used: fewer steps to K within 1e-3 of the converged value
+    than LBFlow's start from rest, the same converged K, no fallback.  The
+    run with the in-run correction (DarcyAccelerator, no network) is timed
+    beside them and printed: it reaches the band sooner than either start."""
+    from lbflow_b200 import Engine
+    from lbflow_b200 import warmstart as ws
+    from lbflow_b200.geometry import porous_medium
+    from lbflow_b200.permeability import converge, time_to_band
+    net, _ = ws.load_mobility(MOB_WEIGHTS)
+    fluid = porous_medium((128, 128, 128), sigma=3.0, porosity=0.22, seed=424242)
+    geom = np.where(fluid, 75, 255).astype(np.uint8)
+    fl = torch.from_numpy(fluid).cuda()
+    runs = {}
+    for mode in ('cold', 'learned', 'correction'):
+        with Engine(geom, LABELS, collision='MRT', tau=(1.0,)) as e:
+            warm = (lambda: ws.mobility_start(e, net, fl, 1.0, 1e-5)) if mode == 'learned' else None
+            acc = ws.DarcyAccelerator(e, fl, 1e-5, block=2, at=(500,)) if mode == 'correction' else None
+            runs[mode] = converge(e, 1.0, 1e-5, report=250, tol=1e-6, max_steps=200000, warm=warm,
+                                  accelerate=acc)
+    K = runs['cold']['K']
+    band = {m: time_to_band(r['history'], K) for m, r in runs.items()}
+    print('steps to the 1e-3 band: ' + ', '.join(f'{m} {b[0] if b else None}' for m, b in band.items()))
+    assert runs['learned']['converged'] and not runs['learned']['fallback']
+    assert abs(runs['learned']['K'] - K) <= 1e-5 * abs(K)
+    assert band['learned'] is not None and band['learned'][0] < band['cold'][0]
+
+
 def test_block_sums_match_dense_macros():
     from lbflow_b200 import Engine
     from lbflow_b200.geometry import porous_medium
