@@ -874,41 +874,52 @@ def operator_run(args):
                           gpu_launches=None, clocks=clocks)))
     return 0
 
-def end_to_end(geometry, args, device):
+def end_to_end(geometry, args, device, repeats=3):
     """Same metric through the C ABI with host buffers: the uint8 geometry
     from the host (classified on the device), initialization, K steps each
     followed by the read-back of the step's flux and mass sums (the numbers
     K is computed from), then the final density and velocity fields in the
     VTI layout into page-locked host memory.  The page-locked output buffer
-    is allocated before the timed region, as a caller reusing it would."""
+    is allocated before the timed region, as a caller reusing it would.
+    Repeated `repeats` times with a fresh engine each; the median run is
+    reported, with the seconds of its phases."""
     from lbflow_b200 import Engine, HostBuffer
     import torch
     fields = HostBuffer(4 * geometry.size)
+    fields.array[::512] = 0.0          # touch the pages before timing
     geom = np.ascontiguousarray(geometry)
-    torch.cuda.synchronize()
-    t = time.perf_counter()
-    eng = Engine(geom, LABELS, model='scsp', collision=args.collision, tau=(1.0,), rho=(1.0,),
-                 storage=args.storage, device=device)
-    eng.initialize()
-    sums = None
-    for _ in range(args.steps):
-        eng.step(1, macros=True)
-        sums = eng.flux_sums()
-    eng.fields_dense_async(fields.ptr.value, fields.count)
-    eng.synchronize()
-    eng.check()
-    dt = time.perf_counter() - t
-    nf = eng.fluid_nodes
-    eng.close()
-    ok = bool(np.isfinite(fields.array[::4097]).all()) and sums is not None and np.isfinite(sums).all()
+    runs = []
+    for _ in range(repeats):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        eng = Engine(geom, LABELS, model='scsp', collision=args.collision, tau=(1.0,), rho=(1.0,),
+                     storage=args.storage, device=device)
+        t1 = time.perf_counter()
+        eng.initialize()
+        sums = None
+        for _ in range(args.steps):
+            eng.step(1, macros=True)
+            sums = eng.flux_sums()
+        t2 = time.perf_counter()
+        eng.fields_dense_async(fields.ptr.value, fields.count)
+        eng.synchronize()
+        eng.check()
+        t3 = time.perf_counter()
+        nf = eng.fluid_nodes
+        eng.close()
+        ok = bool(np.isfinite(fields.array[::4097]).all()) and sums is not None and np.isfinite(sums).all()
+        if not ok:
+            raise RuntimeError('end-to-end run produced non-finite output')
+        runs.append(dict(seconds=t3 - t, create=t1 - t, steps=t2 - t1, fields=t3 - t2))
     fields.close()
-    if not ok:
-        raise RuntimeError('end-to-end run produced non-finite output')
+    runs.sort(key=lambda r: r['seconds'])
+    med = runs[len(runs) // 2]
     h2d = geometry.nbytes + 256 * 24
     d2h = 9 * 8 * args.steps + 4 * 8 * geometry.size
-    return dict(value=nf * args.steps / dt / 1e6, unit='MLUPS',
+    return dict(value=nf * args.steps / med['seconds'] / 1e6, unit='MLUPS',
                 h2d_bytes_per_step=h2d / args.steps, d2h_bytes_per_step=d2h / args.steps,
-                seconds=dt)
+                seconds=med['seconds'], phases={k: med[k] for k in ('create', 'steps', 'fields')},
+                repeats=repeats, seconds_all=[r['seconds'] for r in runs])
 
 
 if __name__ == '__main__':

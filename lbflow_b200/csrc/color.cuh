@@ -3,9 +3,10 @@
 // A step needs the phase field phi = (rho0 - rho1)/rho of every neighbour
 // after streaming, so it runs as two launches over the fluid nodes:
 //   pass 1  color_phase:   pull both components (with bounce-back), write phi;
+//   pass 1b color_grad:    color gradient (legacy interior stencil or the
+//                          geometric wall rotation) from phi;
 //   pass 2  color_collide: pull again, macros, collision of the total
-//           distribution, color gradient (legacy interior stencil or the
-//           geometric wall rotation), perturbation and recoloring.
+//           distribution, perturbation and recoloring.
 // Solid voxels read as phi = 86 (SOLID_DENS_N, colorfluid.cpp:49).
 #pragma once
 #include <type_traits>
@@ -76,7 +77,8 @@ template <class L, class H> struct ColorPacked {
     {
         const float g = (fT - (float)L::w36f(q) * (1.0f / 36.0f) * rho_bar) * ShiftScale<L>::scale(q);
         fout[off] = sr ? from_f_sr(g, r1) : from_f_rn(g);
-        const float share = fabsf(fT) > 1e-30f ? a0 / fT : 0.5f;
+        // The share only needs 2^-15: the fast approximate division is enough.
+        const float share = fabsf(fT) > 1e-30f ? __fdividef(a0, fT) : 0.5f;
         float c = (share + 0.5f) * 32768.0f + (sr ? (float)(r2 >> 8) * (1.0f / 16777216.0f) : 0.5f);
         c = fminf(fmaxf(c, 0.0f), 65535.0f);
         fout[nblk + off] = (uint16_t)c;
@@ -213,72 +215,25 @@ color_phase(const Grid g, const Film film, const typename S::T* __restrict__ fin
     if (!isfinite(d0) || !isfinite(d1) || !isfinite(dt) || !(dt > R(0))) atomicOr(err, kErrDensity);
     // The reference's roundoff allowance, -1e-10 rho (colorfluid.cpp:258), is
     // about 450 FP64 ulps; at FP32 arithmetic the same 450 ulps is 2.7e-5 rho.
-    const R tol = sizeof(R) == 8 ? R(1e-10) : R(2.7e-5);
+    // 16-bit storage quantises each component share to 2^-15 (a density
+    // noise of about 1e-5 rho), so its allowance is 1e-3 rho.
+    const R tol = sizeof(R) == 8 ? R(1e-10) : (IsPacked<S>::value ? R(1e-3) : R(2.7e-5));
     if (d0 < -tol * dt || d1 < -tol * dt) atomicOr(err, kErrComponent);
     phi[i] = (double)((d0 - d1) / dt);
 }
 
-// Pass 2 for one node whose incoming populations f0, f1 (and the neighbour
-// indices nbr) are gathered: macros, collision, gradient, perturbation and
-// recoloring.  COLL: 0 = SRT, 1 = MRT.
-template <class L, class S, int COLL>
-__device__ __forceinline__ void color_update(const Grid& g, const Force& F, const ColorParams& P,
-                                             const ColorWall& W, typename S::T* __restrict__ fout,
-                                             const double* __restrict__ phi, const Macros& mo, const int out,
-                                             uint32_t* __restrict__ err, const uint32_t i,
-                                             typename S::R (&f0)[L::Q], typename S::R (&f1)[L::Q],
-                                             const uint32_t (&nbr)[L::Q])
+// ColorFluid::colorGradient of node i (colorfluid.cpp:435-570) from the
+// phase field of its neighbours (nbr[q]: compact index of x + e_q, or
+// UINT32_MAX for a solid voxel): gr in the reference component order
+// {z,y,x} / {y,x}, after the geometric wall rotation at wall nodes, and the
+// norm of the unrotated gradient.  Non-contracted IEEE operations in the
+// reference's order: the rotation angle is undefined when the in-plane
+// gradient vanishes, so exact cancellations must stay exact.
+template <class L, class R>
+__device__ __forceinline__ void color_gradient_node(const ColorWall& W, const double* __restrict__ phi,
+                                                    const uint32_t i, const R phi_i, const uint32_t (&nbr)[L::Q],
+                                                    R (&gr)[3], R& norm)
 {
-    using R = typename S::R;
-    // ColorFluid::calcMacroVar (colorfluid.cpp:238-290) and bodyForce (:736-750).
-    // The total distribution fT = f0 + f1 is formed first; afterwards only
-    // fT and the two component densities stay live (register budget).
-    R d0 = f0[0], d1 = f1[0];
-#pragma unroll
-    for (int q = 1; q < L::Q; ++q) { d0 += f0[q]; d1 += f1[q]; }
-    R fT[L::Q];
-#pragma unroll
-    for (int q = 0; q < L::Q; ++q) fT[q] = f0[q] + f1[q];
-    const R dt = d0 + d1;
-    const R phi_i = (d0 - d1) / dt;
-    const R tau = (R(1) + phi_i) * R(P.relax0) + (R(1) - phi_i) * R(P.relax1);
-    if (!isfinite(tau) || !(tau > R(0.5))) atomicOr(err, kErrTau);
-    R Fv[3];
-    if (F.uniform) { Fv[0] = R(F.fx); Fv[1] = R(F.fy); Fv[2] = R(F.fz); }
-    else {
-        const double* lf = F.label_force + 3 * __ldg(&F.label[i]);
-        Fv[0] = R(lf[0]); Fv[1] = R(lf[1]); Fv[2] = R(lf[2]);
-    }
-    // Velocity components accumulated in the reference's component order.
-    R u[3] = {R(0), R(0), R(0)};
-#pragma unroll
-    for (int a = 0; a < L::D; ++a) {
-        R v = R(0);
-#pragma unroll
-        for (int q = 1; q < L::Q; ++q) {
-            const int e = comp<L>(q, a);
-            if (e == 1) v += fT[q];
-            else if (e == -1) v -= fT[q];
-        }
-        u[a] = v / dt;
-    }
-    if (!isfinite(u[0]) || !isfinite(u[1]) || !isfinite(u[2])) atomicOr(err, kErrVelocity);
-#pragma unroll
-    for (int a = 0; a < L::D; ++a) u[a] += Fv[a] * R(0.5) / dt;
-
-    if (out & kOutMacros) {
-        mo.rho0[i] = (double)d0;
-        mo.rho1[i] = (double)d1;
-        mo.ind[i] = (double)phi_i;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) mo.u[(size_t)a * g.nfp + i] = (double)u[a];
-    }
-    if (out & kOutAdjacent) {
-        mo.indadj[i] = (double)phi_i;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) mo.uadj[(size_t)a * g.nfp + i] = (double)u[a];
-    }
-
     // ColorFluid::colorGradient (colorfluid.cpp:435-570), gradient in the
     // reference component order gr[0..D-1] = {z,y,x} / {y,x}; it only needs
     // the neighbours' phase field, so it is done before the collision and
@@ -286,7 +241,7 @@ __device__ __forceinline__ void color_update(const Grid& g, const Force& F, cons
     // use non-contracted IEEE operations in the reference's order: the
     // rotation angle is undefined when the in-plane gradient vanishes, so
     // exact cancellations must stay exact.
-    R gr[3] = {R(0), R(0), R(0)};
+    gr[0] = gr[1] = gr[2] = R(0);
     const uint16_t wid = __ldg(&W.angle_id[i]);
     R phin[L::Q];
 #pragma unroll
@@ -311,7 +266,7 @@ __device__ __forceinline__ void color_update(const Grid& g, const Force& F, cons
     for (int d = 0; d < L::D; ++d) gr[d] = xmul(gr[d], R(3));
 #pragma unroll
     for (int d = 0; d < L::D; ++d) n2 = xadd(n2, xmul(gr[d], gr[d]));
-    const R norm = sqrt(n2);
+    norm = sqrt(n2);
     if (wid) {
         const double* cs = W.angles + 2 * wid;
         const R cA = R(cs[0]), sA = R(cs[1]);
@@ -370,6 +325,75 @@ __device__ __forceinline__ void color_update(const Grid& g, const Force& F, cons
             gr[0] = g0; gr[1] = g1;
         }
     }
+
+}
+
+// Pass 2 for one node whose incoming populations f0, f1 (and the neighbour
+// indices nbr) are gathered: macros, collision, gradient, perturbation and
+// recoloring.  COLL: 0 = SRT, 1 = MRT.
+template <class L, class S, int COLL>
+__device__ __forceinline__ void color_update(const Grid& g, const Force& F, const ColorParams& P,
+                                             typename S::T* __restrict__ fout,
+                                             const double* __restrict__ grad, const Macros& mo, const int out,
+                                             uint32_t* __restrict__ err, const uint32_t i,
+                                             typename S::R (&f0)[L::Q], typename S::R (&f1)[L::Q])
+{
+    using R = typename S::R;
+    // ColorFluid::calcMacroVar (colorfluid.cpp:238-290) and bodyForce (:736-750).
+    // The total distribution fT = f0 + f1 is formed first; afterwards only
+    // fT and the two component densities stay live (register budget).
+    R d0 = f0[0], d1 = f1[0];
+#pragma unroll
+    for (int q = 1; q < L::Q; ++q) { d0 += f0[q]; d1 += f1[q]; }
+    R fT[L::Q];
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) fT[q] = f0[q] + f1[q];
+    const R dt = d0 + d1;
+    const R phi_i = (d0 - d1) / dt;
+    const R tau = (R(1) + phi_i) * R(P.relax0) + (R(1) - phi_i) * R(P.relax1);
+    if (!isfinite(tau) || !(tau > R(0.5))) atomicOr(err, kErrTau);
+    R Fv[3];
+    if (F.uniform) { Fv[0] = R(F.fx); Fv[1] = R(F.fy); Fv[2] = R(F.fz); }
+    else {
+        const double* lf = F.label_force + 3 * __ldg(&F.label[i]);
+        Fv[0] = R(lf[0]); Fv[1] = R(lf[1]); Fv[2] = R(lf[2]);
+    }
+    // Velocity components accumulated in the reference's component order.
+    R u[3] = {R(0), R(0), R(0)};
+#pragma unroll
+    for (int a = 0; a < L::D; ++a) {
+        R v = R(0);
+#pragma unroll
+        for (int q = 1; q < L::Q; ++q) {
+            const int e = comp<L>(q, a);
+            if (e == 1) v += fT[q];
+            else if (e == -1) v -= fT[q];
+        }
+        u[a] = v / dt;
+    }
+    if (!isfinite(u[0]) || !isfinite(u[1]) || !isfinite(u[2])) atomicOr(err, kErrVelocity);
+#pragma unroll
+    for (int a = 0; a < L::D; ++a) u[a] += Fv[a] * R(0.5) / dt;
+
+    if (out & kOutMacros) {
+        mo.rho0[i] = (double)d0;
+        mo.rho1[i] = (double)d1;
+        mo.ind[i] = (double)phi_i;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) mo.u[(size_t)a * g.nfp + i] = (double)u[a];
+    }
+    if (out & kOutAdjacent) {
+        mo.indadj[i] = (double)phi_i;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) mo.uadj[(size_t)a * g.nfp + i] = (double)u[a];
+    }
+
+    // The colour gradient of this step (color_grad, from the phase field of
+    // pass 1): gr in the reference component order, then the norm.
+    R gr[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) gr[d] = R(__ldg(&grad[(size_t)d * g.nfp + i]));
+    const R norm = R(__ldg(&grad[(size_t)3 * g.nfp + i]));
 
     // ColorFluid::collision (colorfluid.cpp:334-387): collide the total
     // fT towards feq = feq_u0 + rho w (3 e.u + 4.5 (e.u)^2 - 1.5 u^2),
@@ -442,16 +466,38 @@ __device__ __forceinline__ void color_update(const Grid& g, const Force& F, cons
     }
 }
 
-// Pass 2: collision, gradient, perturbation and recoloring of every fluid node.
-// PULL = false is the t = 0 collision.
-// At most 128 registers per thread (four 128-thread blocks per SM): the
-// kernel is latency-bound, and the FP64 D3Q19 form otherwise needs 132
-// registers, which leaves three blocks per SM (measured 12 % slower).
+// Pass 1b: the colour gradient of every fluid node from the phase field of
+// pass 1, written as grad[4][nfp] (gr in the reference component order, then
+// the norm).  Kept out of pass 2 so that pass 2 holds neither the
+// neighbours' phase values nor the wall rotation in registers.
+template <class L, class R>
+__global__ void __launch_bounds__(128)
+color_grad(const Grid g, const ColorWall W, const double* __restrict__ phi, double* __restrict__ grad)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.nf) return;
+    int x, y, z;
+    unpack(__ldg(&g.coord[i]), x, y, z);
+    uint32_t src[L::Q], nbr[L::Q];
+    const uint32_t mask = pull_sources<L>(g, x, y, z, src);
+    nbr[0] = i;
+#pragma unroll
+    for (int q = 1; q < L::Q; ++q) nbr[L::op(q)] = (mask >> q) & 1u ? src[q] : 0xffffffffu;
+    R gr[3], norm;
+    color_gradient_node<L, R>(W, phi, i, R(__ldg(&phi[i])), nbr, gr, norm);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) grad[(size_t)d * g.nfp + i] = (double)gr[d];
+    grad[(size_t)3 * g.nfp + i] = (double)norm;
+}
+
+// Pass 2: collision, perturbation and recoloring of every fluid node.
+// PULL = false is the t = 0 collision.  At most 128 registers per thread
+// (four 128-thread blocks per SM): the kernel is latency-bound.
 template <class L, class S, int COLL, bool PULL, bool FILM>
 __global__ void __launch_bounds__(128, 4)
-color_collide(const Grid g, const Film film, const Force F, const ColorParams P, const ColorWall W,
+color_collide(const Grid g, const Film film, const Force F, const ColorParams P,
               const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
-              const double* __restrict__ phi, Macros mo, const int out, uint32_t* __restrict__ err)
+              const double* __restrict__ grad, Macros mo, const int out, uint32_t* __restrict__ err)
 {
     using R = typename S::R;
     // Blocks run in descending node order: pass 1 has just read the
@@ -465,17 +511,7 @@ color_collide(const Grid g, const Film film, const Force F, const ColorParams P,
     R f0[L::Q], f1[L::Q];
     uint32_t nbr[L::Q];
     color_gather<L, S, PULL, FILM>(g, film, fin, i, x, y, z, f0, f1, nbr, R(P.rho_ref[0]));
-    if (!PULL) {
-        // t = 0: neighbours by direct lookup (the pull above read local values).
-#pragma unroll
-        for (int q = 1; q < L::Q; ++q) {
-            bool fluid;
-            const uint32_t j = lookup(g, wrap(x + L::ex(q), g.nx), wrap(y + L::ey(q), g.ny),
-                                      L::D == 3 ? wrap(z + L::ez(q), g.nz) : 0, fluid);
-            nbr[q] = fluid ? j : 0xffffffffu;
-        }
-    }
-    color_update<L, S, COLL>(g, F, P, W, fout, phi, mo, out, err, i, f0, f1, nbr);
+    color_update<L, S, COLL>(g, F, P, fout, grad, mo, out, err, i, f0, f1);
 }
 
 // ---- two-phase Zou-He boundaries ------------------------------------------------
@@ -592,7 +628,7 @@ color_zou_he_phase(const Grid g, const Film film, const ZouHe z, const typename 
     for (int q = 1; q < L::Q; ++q) { d0 += f0[q]; d1 += f1[q]; }
     const R dt = d0 + d1;
     if (!isfinite(d0) || !isfinite(d1) || !isfinite(dt) || !(dt > R(0))) atomicOr(err, kErrDensity);
-    const R tol = sizeof(R) == 8 ? R(1e-10) : R(2.7e-5);
+    const R tol = sizeof(R) == 8 ? R(1e-10) : (IsPacked<S>::value ? R(1e-3) : R(2.7e-5));
     if (d0 < -tol * dt || d1 < -tol * dt) atomicOr(err, kErrComponent);
     phi[i] = (double)((d0 - d1) / dt);
 }
@@ -602,10 +638,9 @@ color_zou_he_phase(const Grid g, const Film film, const ZouHe z, const typename 
 // rho0 - rho1 of the last step that asked for the adjacent history.
 template <class L, class S, int COLL, bool FILM>
 __global__ void __launch_bounds__(128)
-color_zou_he_collide(const Grid g, const Film film, const Force F, const ColorParams P, const ColorWall W,
-                     const ZouHe z,
+color_zou_he_collide(const Grid g, const Film film, const Force F, const ColorParams P, const ZouHe z,
                      const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
-                     const double* __restrict__ phi, Macros mo, const int out, uint32_t* __restrict__ err)
+                     const double* __restrict__ grad, Macros mo, const int out, uint32_t* __restrict__ err)
 {
     using R = typename S::R;
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -618,7 +653,7 @@ color_zou_he_collide(const Grid g, const Film film, const Force F, const ColorPa
     R d0 = f0[0], d1 = f1[0];
 #pragma unroll
     for (int q = 1; q < L::Q; ++q) { d0 += f0[q]; d1 += f1[q]; }
-    color_update<L, S, COLL>(g, F, P, W, fout, phi, mo, out, err, i, f0, f1, nbr);
+    color_update<L, S, COLL>(g, F, P, fout, grad, mo, out, err, i, f0, f1);
     if (out & kOutMacros) {
         const double prev = z.num[k];
         mo.indadj[i] = (double)dens > 0.0 ? prev / (double)dens : 0.0;
