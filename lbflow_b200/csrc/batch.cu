@@ -164,6 +164,7 @@ struct lbf_batch {
     double* d_out = nullptr;
     uint32_t* d_step = nullptr;       // pull-step count, two words by buffer parity (FP16 rounding seeds)
     uint32_t ntiles_all = 0, ntiles_active = 0;
+    size_t tile_cap = 0;              // capacity of the device tile arrays
     std::vector<Tile> tiles_all;
     std::vector<uint32_t> tile_first, tile_count;
     Force force{};
@@ -251,16 +252,23 @@ int build_tiles(lbf_batch* b)
         b->tile_count[g] = (uint32_t)b->tiles_all.size() - b->tile_first[g];
     }
     b->ntiles_all = (uint32_t)b->tiles_all.size();
-    cudaFree(b->d_tiles_all); cudaFree(b->d_tiles_active); cudaFree(b->d_partial);
-    cudaFree(b->d_tile_first); cudaFree(b->d_tile_count);
-    b->d_tiles_all = b->d_tiles_active = nullptr;
-    b->d_partial = nullptr;
+    // Device tile arrays grow only (retiring geometries inside a run, which
+    // rebuilds the active schedule, then makes no allocation).
     const size_t nt = std::max<size_t>(1, b->ntiles_all);
-    BCK(b, cudaMalloc(&b->d_tiles_all, nt * sizeof(Tile)));
-    BCK(b, cudaMalloc(&b->d_tiles_active, nt * sizeof(Tile)));
-    BCK(b, cudaMalloc(&b->d_partial, nt * kReduceMaxK * sizeof(double)));
-    BCK(b, cudaMalloc(&b->d_tile_first, std::max<size_t>(1, b->count) * sizeof(uint32_t)));
-    BCK(b, cudaMalloc(&b->d_tile_count, std::max<size_t>(1, b->count) * sizeof(uint32_t)));
+    if (nt > b->tile_cap) {
+        cudaFree(b->d_tiles_all); cudaFree(b->d_tiles_active); cudaFree(b->d_partial);
+        b->d_tiles_all = b->d_tiles_active = nullptr;
+        b->d_partial = nullptr;
+        b->tile_cap = 0;
+        BCK(b, cudaMalloc(&b->d_tiles_all, nt * sizeof(Tile)));
+        BCK(b, cudaMalloc(&b->d_tiles_active, nt * sizeof(Tile)));
+        BCK(b, cudaMalloc(&b->d_partial, nt * kReduceMaxK * sizeof(double)));
+        b->tile_cap = nt;
+    }
+    if (!b->d_tile_first) {
+        BCK(b, cudaMalloc(&b->d_tile_first, std::max<size_t>(1, b->count) * sizeof(uint32_t)));
+        BCK(b, cudaMalloc(&b->d_tile_count, std::max<size_t>(1, b->count) * sizeof(uint32_t)));
+    }
     BCK(b, cudaMemcpyAsync(b->d_tiles_all, b->tiles_all.data(), b->ntiles_all * sizeof(Tile), cudaMemcpyHostToDevice, b->stream));
     BCK(b, cudaMemcpyAsync(b->d_tile_first, b->tile_first.data(), b->count * sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream));
     BCK(b, cudaMemcpyAsync(b->d_tile_count, b->tile_count.data(), b->count * sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream));

@@ -322,7 +322,7 @@ struct Solver {
         used += (n * sizeof(T) + 255) / 256 * 256;
         return p;
     }
-    ~Solver() { if (base) cudaFree(base); }
+    ~Solver() { if (base) cudaFreeAsync(base, s); }
 
     void smooth(int l, int sweeps)
     {
@@ -391,8 +391,15 @@ extern "C" int lbf_darcy_pressure(const double* mob, uint32_t nz, uint32_t ny, u
     double *rhs = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *Ap = nullptr, *sc = nullptr;
     for (int pass = 0; pass < 2; ++pass) {
         if (pass == 1) {
+            // The workspace comes from the library's device pool on the
+            // solve's stream: a correction inside a timed run reuses memory
+            // reserved by earlier solves instead of calling the driver.
             void* mem = nullptr;
-            S.err = cudaMalloc(&mem, S.used);
+            int dev = 0;
+            cudaMemPool_t pool = nullptr;
+            S.err = cudaGetDevice(&dev);
+            if (S.err == cudaSuccess) S.err = lbf::device_pool(dev, &pool);
+            if (S.err == cudaSuccess) S.err = cudaMallocFromPoolAsync(&mem, S.used, pool, S.s);
             if (S.err != cudaSuccess)
                 return fail(std::string("lbf_darcy_pressure: ") + cudaGetErrorString(S.err), LBF_ENOMEM);
             S.base = static_cast<char*>(mem);

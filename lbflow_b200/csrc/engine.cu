@@ -90,7 +90,9 @@ constexpr uint64_t kPoolKeepBytes = 8ull << 30;
 std::mutex g_pool_mu;
 cudaMemPool_t g_pool[64] = {};
 
-cudaError_t engine_pool(int device, cudaMemPool_t* pool)
+}  // namespace
+
+cudaError_t lbf::device_pool(int device, cudaMemPool_t* pool)
 {
     if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lock(g_pool_mu);
@@ -110,6 +112,10 @@ cudaError_t engine_pool(int device, cudaMemPool_t* pool)
     *pool = g_pool[device];
     return cudaSuccess;
 }
+
+namespace {
+
+cudaError_t engine_pool(int device, cudaMemPool_t* pool) { return lbf::device_pool(device, pool); }
 
 template <class T>
 int dalloc(lbf_engine* e, T** p, size_t count)

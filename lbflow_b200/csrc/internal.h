@@ -52,6 +52,11 @@ void launch_color(int dims, int storage, int collision, bool pull, int out, cons
 void launch_color_init(int dims, int storage, const Grid& g, const Force& F, const ColorParams& P,
                        const uint8_t* phase, void* f, cudaStream_t s);
 
+// The library's stream-ordered device memory pool of a device (created on
+// first use; keeps freed memory reserved for reuse up to a fixed amount), so
+// that work repeated inside a run allocates without driver calls.
+cudaError_t device_pool(int device, cudaMemPool_t* pool);
+
 // Message returned by lbf_last_error(NULL) (calls without an engine).
 void set_global_error(const std::string& msg);
 
