@@ -198,7 +198,7 @@ template <class L> constexpr int normal_codes() { return L::D == 3 ? 11 * 11 * 1
 template <class L, class S, bool PULL, bool FILM>
 __global__ void __launch_bounds__(128)
 color_phase(const Grid g, const Film film, const typename S::T* __restrict__ fin, double* __restrict__ phi,
-            uint32_t* __restrict__ err, const double rho_bar)
+            double* __restrict__ phid, uint32_t* __restrict__ err, const double rho_bar)
 {
     using R = typename S::R;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -219,20 +219,21 @@ color_phase(const Grid g, const Film film, const typename S::T* __restrict__ fin
     // noise of about 1e-5 rho), so its allowance is 1e-3 rho.
     const R tol = sizeof(R) == 8 ? R(1e-10) : (IsPacked<S>::value ? R(1e-3) : R(2.7e-5));
     if (d0 < -tol * dt || d1 < -tol * dt) atomicOr(err, kErrComponent);
-    phi[i] = (double)((d0 - d1) / dt);
+    const double ph = (double)((d0 - d1) / dt);
+    phi[i] = ph;
+    phid[((size_t)z * g.ny + y) * g.nx + x] = ph;
 }
 
 // ColorFluid::colorGradient of node i (colorfluid.cpp:435-570) from the
-// phase field of its neighbours (nbr[q]: compact index of x + e_q, or
-// UINT32_MAX for a solid voxel): gr in the reference component order
-// {z,y,x} / {y,x}, after the geometric wall rotation at wall nodes, and the
-// norm of the unrotated gradient.  Non-contracted IEEE operations in the
-// reference's order: the rotation angle is undefined when the in-plane
-// gradient vanishes, so exact cancellations must stay exact.
+// phase field of its neighbours (phin[q]: phi at x + e_q, kSolidPhi for a
+// solid voxel): gr in the reference component order {z,y,x} / {y,x}, after
+// the geometric wall rotation at wall nodes, and the norm of the unrotated
+// gradient.  Non-contracted IEEE operations in the reference's order: the
+// rotation angle is undefined when the in-plane gradient vanishes, so exact
+// cancellations must stay exact.
 template <class L, class R>
-__device__ __forceinline__ void color_gradient_node(const ColorWall& W, const double* __restrict__ phi,
-                                                    const uint32_t i, const R phi_i, const uint32_t (&nbr)[L::Q],
-                                                    R (&gr)[3], R& norm)
+__device__ __forceinline__ void color_gradient_node(const ColorWall& W, const uint32_t i, const R phi_i,
+                                                    const R (&phin)[L::Q], R (&gr)[3], R& norm)
 {
     // ColorFluid::colorGradient (colorfluid.cpp:435-570), gradient in the
     // reference component order gr[0..D-1] = {z,y,x} / {y,x}; it only needs
@@ -243,9 +244,6 @@ __device__ __forceinline__ void color_gradient_node(const ColorWall& W, const do
     // exact cancellations must stay exact.
     gr[0] = gr[1] = gr[2] = R(0);
     const uint16_t wid = __ldg(&W.angle_id[i]);
-    R phin[L::Q];
-#pragma unroll
-    for (int q = 1; q < L::Q; ++q) phin[q] = nbr[q] == 0xffffffffu ? R(kSolidPhi) : R(__ldg(&phi[nbr[q]]));
 #pragma unroll
     for (int d = 0; d < L::D; ++d) {
 #pragma unroll
@@ -273,7 +271,7 @@ __device__ __forceinline__ void color_gradient_node(const ColorWall& W, const do
         int nn[3] = {0, 0, 0};   // normal in reference order
 #pragma unroll
         for (int q = 1; q < L::Q; ++q)
-            if (nbr[q] == 0xffffffffu) {
+            if (phin[q] == R(kSolidPhi)) {
 #pragma unroll
                 for (int d = 0; d < L::D; ++d) nn[d] -= comp<L>(q, L::D - 1 - d);
             }
@@ -469,22 +467,29 @@ __device__ __forceinline__ void color_update(const Grid& g, const Force& F, cons
 // Pass 1b: the colour gradient of every fluid node from the phase field of
 // pass 1, written as grad[4][nfp] (gr in the reference component order, then
 // the norm).  Kept out of pass 2 so that pass 2 holds neither the
-// neighbours' phase values nor the wall rotation in registers.
+// neighbours' phase values nor the wall rotation in registers.  The phase
+// field is read from its dense voxel copy (pass 1 writes both; solid voxels
+// hold kSolidPhi, SOLID_DENS_N of colorfluid.cpp:49), so a neighbour is one
+// address computation instead of an occupancy lookup.
 template <class L, class R>
 __global__ void __launch_bounds__(128)
-color_grad(const Grid g, const ColorWall W, const double* __restrict__ phi, double* __restrict__ grad)
+color_grad(const Grid g, const ColorWall W, const double* __restrict__ phid, double* __restrict__ grad)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= g.nf) return;
     int x, y, z;
     unpack(__ldg(&g.coord[i]), x, y, z);
-    uint32_t src[L::Q], nbr[L::Q];
-    const uint32_t mask = pull_sources<L>(g, x, y, z, src);
-    nbr[0] = i;
+    const int xs[3] = {x == 0 ? g.nx - 1 : x - 1, x, x + 1 == g.nx ? 0 : x + 1};
+    const int ys[3] = {y == 0 ? g.ny - 1 : y - 1, y, y + 1 == g.ny ? 0 : y + 1};
+    const int zs[3] = {z == 0 ? g.nz - 1 : z - 1, z, z + 1 == g.nz ? 0 : z + 1};
+    R phin[L::Q];
 #pragma unroll
-    for (int q = 1; q < L::Q; ++q) nbr[L::op(q)] = (mask >> q) & 1u ? src[q] : 0xffffffffu;
+    for (int q = 0; q < L::Q; ++q) {
+        const size_t v = ((size_t)zs[1 + L::ez(q)] * g.ny + ys[1 + L::ey(q)]) * g.nx + xs[1 + L::ex(q)];
+        phin[q] = R(__ldg(&phid[v]));
+    }
     R gr[3], norm;
-    color_gradient_node<L, R>(W, phi, i, R(__ldg(&phi[i])), nbr, gr, norm);
+    color_gradient_node<L, R>(W, i, phin[0], phin, gr, norm);
 #pragma unroll
     for (int d = 0; d < 3; ++d) grad[(size_t)d * g.nfp + i] = (double)gr[d];
     grad[(size_t)3 * g.nfp + i] = (double)norm;
@@ -613,7 +618,8 @@ __device__ __forceinline__ void color_zou_he_gather(const Grid& g, const Film& f
 template <class L, class S, bool FILM>
 __global__ void __launch_bounds__(128)
 color_zou_he_phase(const Grid g, const Film film, const ZouHe z, const typename S::T* __restrict__ fin,
-                   double* __restrict__ phi, uint32_t* __restrict__ err, const double rho_bar)
+                   double* __restrict__ phi, double* __restrict__ phid, uint32_t* __restrict__ err,
+                   const double rho_bar)
 {
     using R = typename S::R;
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -630,7 +636,11 @@ color_zou_he_phase(const Grid g, const Film film, const ZouHe z, const typename 
     if (!isfinite(d0) || !isfinite(d1) || !isfinite(dt) || !(dt > R(0))) atomicOr(err, kErrDensity);
     const R tol = sizeof(R) == 8 ? R(1e-10) : (IsPacked<S>::value ? R(1e-3) : R(2.7e-5));
     if (d0 < -tol * dt || d1 < -tol * dt) atomicOr(err, kErrComponent);
-    phi[i] = (double)((d0 - d1) / dt);
+    const double ph = (double)((d0 - d1) / dt);
+    phi[i] = ph;
+    int vx, vy, vz;
+    unpack(__ldg(&g.coord[i]), vx, vy, vz);
+    phid[((size_t)vz * g.ny + vy) * g.nx + vx] = ph;
 }
 
 // Boundary collision pass (after pass 2); also keeps the report's adjacent

@@ -30,6 +30,7 @@ struct ColorLaunch {
     const void* fin;   // [2][Q][nfp]
     void* fout;
     double* phi;       // [nfp] phase field of this step (written by pass 1)
+    double* phid;      // [N] the same phase field per voxel (solid voxels: kSolidPhi)
     double* grad;      // [4][nfp] colour gradient (z,y,x / y,x order) and its norm (pass 1b)
     Macros mo;
     uint32_t* err;
