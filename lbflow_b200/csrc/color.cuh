@@ -2,11 +2,11 @@
 //
 // A step needs the phase field phi = (rho0 - rho1)/rho of every neighbour
 // after streaming, so it runs as two launches over the fluid nodes:
-//   pass 1  color_phase:   pull both components (with bounce-back), write phi;
-//   pass 1b color_grad:    color gradient (legacy interior stencil or the
-//                          geometric wall rotation) from phi;
-//   pass 2  color_collide: pull again, macros, collision of the total
-//           distribution, perturbation and recoloring.
+//   pass 1  color_phase:   pull both components (with bounce-back), write phi
+//                          (compact and as a dense per-voxel copy);
+//   pass 2  color_collide: color gradient from the dense phi (legacy interior
+//           stencil or the geometric wall rotation), pull again, macros,
+//           collision of the total distribution, perturbation and recoloring.
 // Solid voxels read as phi = 86 (SOLID_DENS_N, colorfluid.cpp:49).
 #pragma once
 #include <type_traits>
@@ -250,13 +250,14 @@ __device__ __forceinline__ void color_gradient_node(const ColorWall& W, const ui
         for (int k = 0; k < L::NRELD; ++k) {
             const int q = L::reld(d, k);
             const int e = comp<L>(q, L::D - 1 - d);
-            R term = phin[q];
-            if (wid) {
-                if (phin[q] == R(kSolidPhi)) continue;
-                term = xsub(phin[q], phi_i);
-            }
-            if (e == 1) gr[d] = xadd(gr[d], xmul(R(w<L>(q)), term));
-            else gr[d] = xsub(gr[d], xmul(R(w<L>(q)), term));
+            // Interior: the neighbour's phi; wall node: phi difference over
+            // fluid neighbours only (a solid neighbour's term is skipped).
+            // Selects instead of branches: the warp's lanes mix both kinds.
+            const bool skip = wid && phin[q] == R(kSolidPhi);
+            const R term = wid ? xsub(phin[q], phi_i) : phin[q];
+            const R c = xmul(R(w<L>(q)), term);
+            const R nv = e == 1 ? xadd(gr[d], c) : xsub(gr[d], c);
+            gr[d] = skip ? gr[d] : nv;
         }
     }
     R n2 = R(0);
@@ -332,7 +333,8 @@ __device__ __forceinline__ void color_gradient_node(const ColorWall& W, const ui
 template <class L, class S, int COLL>
 __device__ __forceinline__ void color_update(const Grid& g, const Force& F, const ColorParams& P,
                                              typename S::T* __restrict__ fout,
-                                             const double* __restrict__ grad, const Macros& mo, const int out,
+                                             const typename S::R (&gr)[3], const typename S::R norm,
+                                             const Macros& mo, const int out,
                                              uint32_t* __restrict__ err, const uint32_t i,
                                              typename S::R (&f0)[L::Q], typename S::R (&f1)[L::Q])
 {
@@ -385,13 +387,6 @@ __device__ __forceinline__ void color_update(const Grid& g, const Force& F, cons
 #pragma unroll
         for (int a = 0; a < 3; ++a) mo.uadj[(size_t)a * g.nfp + i] = (double)u[a];
     }
-
-    // The colour gradient of this step (color_grad, from the phase field of
-    // pass 1): gr in the reference component order, then the norm.
-    R gr[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) gr[d] = R(__ldg(&grad[(size_t)d * g.nfp + i]));
-    const R norm = R(__ldg(&grad[(size_t)3 * g.nfp + i]));
 
     // ColorFluid::collision (colorfluid.cpp:334-387): collide the total
     // fT towards feq = feq_u0 + rho w (3 e.u + 4.5 (e.u)^2 - 1.5 u^2),
@@ -464,21 +459,14 @@ __device__ __forceinline__ void color_update(const Grid& g, const Force& F, cons
     }
 }
 
-// Pass 1b: the colour gradient of every fluid node from the phase field of
-// pass 1, written as grad[4][nfp] (gr in the reference component order, then
-// the norm).  Kept out of pass 2 so that pass 2 holds neither the
-// neighbours' phase values nor the wall rotation in registers.  The phase
-// field is read from its dense voxel copy (pass 1 writes both; solid voxels
-// hold kSolidPhi, SOLID_DENS_N of colorfluid.cpp:49), so a neighbour is one
-// address computation instead of an occupancy lookup.
+// Colour gradient of node i at (x, y, z) from the dense per-voxel phase
+// field (solid voxels hold kSolidPhi, SOLID_DENS_N of colorfluid.cpp:49):
+// each neighbour is one address computation, no occupancy lookup.
 template <class L, class R>
-__global__ void __launch_bounds__(128)
-color_grad(const Grid g, const ColorWall W, const double* __restrict__ phid, double* __restrict__ grad)
+__device__ __forceinline__ void color_gradient_dense(const Grid& g, const ColorWall& W,
+                                                     const double* __restrict__ phid, const uint32_t i, int x, int y,
+                                                     int z, R (&gr)[3], R& norm)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.nf) return;
-    int x, y, z;
-    unpack(__ldg(&g.coord[i]), x, y, z);
     const int xs[3] = {x == 0 ? g.nx - 1 : x - 1, x, x + 1 == g.nx ? 0 : x + 1};
     const int ys[3] = {y == 0 ? g.ny - 1 : y - 1, y, y + 1 == g.ny ? 0 : y + 1};
     const int zs[3] = {z == 0 ? g.nz - 1 : z - 1, z, z + 1 == g.nz ? 0 : z + 1};
@@ -488,21 +476,19 @@ color_grad(const Grid g, const ColorWall W, const double* __restrict__ phid, dou
         const size_t v = ((size_t)zs[1 + L::ez(q)] * g.ny + ys[1 + L::ey(q)]) * g.nx + xs[1 + L::ex(q)];
         phin[q] = R(__ldg(&phid[v]));
     }
-    R gr[3], norm;
     color_gradient_node<L, R>(W, i, phin[0], phin, gr, norm);
-#pragma unroll
-    for (int d = 0; d < 3; ++d) grad[(size_t)d * g.nfp + i] = (double)gr[d];
-    grad[(size_t)3 * g.nfp + i] = (double)norm;
 }
 
-// Pass 2: collision, perturbation and recoloring of every fluid node.
-// PULL = false is the t = 0 collision.  At most 128 registers per thread
+// Pass 2: colour gradient, collision, perturbation and recoloring of every
+// fluid node.  PULL = false is the t = 0 collision.  The gradient comes
+// first, from the dense phase field (its loads hit L2), while the node's
+// population loads are independent of it.  At most 128 registers per thread
 // (four 128-thread blocks per SM): the kernel is latency-bound.
 template <class L, class S, int COLL, bool PULL, bool FILM>
 __global__ void __launch_bounds__(128, 4)
-color_collide(const Grid g, const Film film, const Force F, const ColorParams P,
+color_collide(const Grid g, const Film film, const Force F, const ColorParams P, const ColorWall W,
               const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
-              const double* __restrict__ grad, Macros mo, const int out, uint32_t* __restrict__ err)
+              const double* __restrict__ phid, Macros mo, const int out, uint32_t* __restrict__ err)
 {
     using R = typename S::R;
     // Blocks run in descending node order: pass 1 has just read the
@@ -513,10 +499,12 @@ color_collide(const Grid g, const Film film, const Force F, const ColorParams P,
     if (i >= g.nf) return;
     int x, y, z;
     unpack(__ldg(&g.coord[i]), x, y, z);
+    R gr[3], norm;
+    color_gradient_dense<L, R>(g, W, phid, i, x, y, z, gr, norm);
     R f0[L::Q], f1[L::Q];
     uint32_t nbr[L::Q];
     color_gather<L, S, PULL, FILM>(g, film, fin, i, x, y, z, f0, f1, nbr, R(P.rho_ref[0]));
-    color_update<L, S, COLL>(g, F, P, fout, grad, mo, out, err, i, f0, f1);
+    color_update<L, S, COLL>(g, F, P, fout, gr, norm, mo, out, err, i, f0, f1);
 }
 
 // ---- two-phase Zou-He boundaries ------------------------------------------------
@@ -648,9 +636,10 @@ color_zou_he_phase(const Grid g, const Film film, const ZouHe z, const typename 
 // rho0 - rho1 of the last step that asked for the adjacent history.
 template <class L, class S, int COLL, bool FILM>
 __global__ void __launch_bounds__(128)
-color_zou_he_collide(const Grid g, const Film film, const Force F, const ColorParams P, const ZouHe z,
+color_zou_he_collide(const Grid g, const Film film, const Force F, const ColorParams P, const ColorWall W,
+                     const ZouHe z,
                      const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
-                     const double* __restrict__ grad, Macros mo, const int out, uint32_t* __restrict__ err)
+                     const double* __restrict__ phid, Macros mo, const int out, uint32_t* __restrict__ err)
 {
     using R = typename S::R;
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -663,7 +652,13 @@ color_zou_he_collide(const Grid g, const Film film, const Force F, const ColorPa
     R d0 = f0[0], d1 = f1[0];
 #pragma unroll
     for (int q = 1; q < L::Q; ++q) { d0 += f0[q]; d1 += f1[q]; }
-    color_update<L, S, COLL>(g, F, P, fout, grad, mo, out, err, i, f0, f1);
+    R gr[3], norm;
+    {
+        int gx, gy, gz;
+        unpack(__ldg(&g.coord[i]), gx, gy, gz);
+        color_gradient_dense<L, R>(g, W, phid, i, gx, gy, gz, gr, norm);
+    }
+    color_update<L, S, COLL>(g, F, P, fout, gr, norm, mo, out, err, i, f0, f1);
     if (out & kOutMacros) {
         const double prev = z.num[k];
         mo.indadj[i] = (double)dens > 0.0 ? prev / (double)dens : 0.0;

@@ -26,16 +26,15 @@ void run_step(bool pull, int out, const ColorLaunch& a)
                                                                      rb);
     if (!pull && zb && (out & kOutAdjacent))
         color_zou_he_record<L, S><<<zb, threads, 0, a.stream>>>(a.g, a.zh, fin, rb);
-    color_grad<L, typename S::R><<<blocks, threads, 0, a.stream>>>(a.g, a.W, a.phid, a.grad);
     if (pull)
         color_collide<L, S, COLL, true, FILM><<<blocks, threads, 0, a.stream>>>(
-            a.g, a.film, a.F, a.P, fin, fout, a.grad, a.mo, out, a.err);
+            a.g, a.film, a.F, a.P, a.W, fin, fout, a.phid, a.mo, out, a.err);
     else
         color_collide<L, S, COLL, false, false><<<blocks, threads, 0, a.stream>>>(
-            a.g, a.film, a.F, a.P, fin, fout, a.grad, a.mo, out, a.err);
+            a.g, a.film, a.F, a.P, a.W, fin, fout, a.phid, a.mo, out, a.err);
     if (pull && zb)
-        color_zou_he_collide<L, S, COLL, FILM><<<zb, threads, 0, a.stream>>>(a.g, a.film, a.F, a.P, a.zh, fin,
-                                                                            fout, a.grad, a.mo, out, a.err);
+        color_zou_he_collide<L, S, COLL, FILM><<<zb, threads, 0, a.stream>>>(a.g, a.film, a.F, a.P, a.W, a.zh, fin,
+                                                                            fout, a.phid, a.mo, out, a.err);
 }
 
 template <class L, class S, int COLL>

@@ -37,7 +37,6 @@ struct lbf_engine {
     double* label_force = nullptr;
     double *rho0 = nullptr, *rho1 = nullptr, *u = nullptr, *uprev = nullptr, *uadj = nullptr;
     double *ind = nullptr, *indprev = nullptr, *indadj = nullptr, *phi = nullptr;
-    double* grad = nullptr;         // color: gradient of the step [4][nfp]
     double* phid = nullptr;         // color: phase field per voxel [N], solid voxels kSolidPhi
     uint16_t* angle_id = nullptr;
     double* angles = nullptr;
@@ -243,7 +242,7 @@ void launch_step(lbf_engine* e, bool pull, int out)
         const bool dither = e->cfg.storage == LBF_STORE_FP16 || e->cfg.storage == LBF_STORE_BF16;
         e->cp.seed = dither && pull ? (++e->steps * 2654435761u) | 1u : 0u;
         ColorWall W{e->angle_id, e->angles, e->tib};
-        ColorLaunch a{grid_of(e), e->force, e->cp, W, fin, fout, e->phi, e->phid, e->grad, macros_of(e), e->err,
+        ColorLaunch a{grid_of(e), e->force, e->cp, W, fin, fout, e->phi, e->phid, macros_of(e), e->err,
                       e->stream, e->zh, Film{{e->film_bits[0], e->film_bits[1]}}};
         launch_color(e->D, (int)e->cfg.storage, (int)e->cfg.collision, pull, out, a);
     }
@@ -1002,7 +1001,6 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
         LBF_ALLOC(e->indprev, e->nfp);
         LBF_ALLOC(e->indadj, e->nfp);
         LBF_ALLOC(e->phi, e->nfp);
-        LBF_ALLOC(e->grad, 4 * (size_t)e->nfp);
         LBF_ALLOC(e->phid, e->N);
         fill_value<<<dense_blocks(e->N), 256, 0, e->stream>>>(e->phid, e->N, kSolidPhi);
         LBF_CUDA(cudaGetLastError());
@@ -1034,7 +1032,7 @@ void lbf_destroy(lbf_engine* e)
                     e->rho0, e->rho1, e->u, e->uprev, e->uadj, e->ind, e->indprev, e->indadj,
                     e->phi, e->angle_id, e->angles, e->tib, e->err, e->partial, e->red,
                     e->zh_node, e->zh_code, e->zh_value, e->zh_num, e->dense_tmp, e->film_bits[0], e->film_bits[1],
-                    e->stage, e->grad, e->phid};
+                    e->stage, e->phid};
     for (void* p : ptrs) if (p) cudaFreeAsync(p, e->stream);
     if (e->stream) cudaStreamSynchronize(e->stream);
     if (e->h_red) cudaFreeHost(e->h_red);

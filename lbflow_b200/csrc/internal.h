@@ -31,7 +31,6 @@ struct ColorLaunch {
     void* fout;
     double* phi;       // [nfp] phase field of this step (written by pass 1)
     double* phid;      // [N] the same phase field per voxel (solid voxels: kSolidPhi)
-    double* grad;      // [4][nfp] colour gradient (z,y,x / y,x order) and its norm (pass 1b)
     Macros mo;
     uint32_t* err;
     cudaStream_t stream;
