@@ -204,6 +204,18 @@ int lbf_get_macros(lbf_engine *e, double *rho0, double *rho1, double *u);
  * value sets LBF_ERR_OUTPUT in the error word (the reference refuses to
  * write such a checkpoint, simulator.cpp:327-333). */
 int lbf_fields_dense_async(lbf_engine *e, double *out, size_t n);
+
+/* Checkpoint compatibility: from now on also carry the populations of solid
+ * voxels, streamed exactly as Simulator::streaming moves every voxel
+ * (simulator.cpp:73-101; solid voxels are never collided, and bounce-back,
+ * simulator.cpp:103-111, keeps their values out of the fluid), so that
+ * lbf_get_populations / lbf_populations_dense_async reproduce saveRst
+ * (scsp.cpp:277-302; colorfluid.cpp:766-812) at solid voxels too, and
+ * lbf_set_populations loads them.  Call before lbf_initialize or
+ * lbf_set_populations; FP64 storage only.  Costs one extra pass over all
+ * voxels per step and 2 * phases * Q * 8 bytes per solid voxel.  Without it
+ * solid entries are written as 0 (they never influence the flow). */
+int lbf_keep_solid_populations(lbf_engine *e);
 int lbf_populations_dense_async(lbf_engine *e, double *out, size_t n);
 
 /* Page-locked host memory the device can write (cudaHostAlloc, portable and

@@ -78,6 +78,7 @@ def library():
             'lbf_create': (I, [ctypes.POINTER(_Config), ctypes.POINTER(_Label), ctypes.c_char_p, ctypes.POINTER(P)]),
             'lbf_destroy': (None, [P]),
             'lbf_initialize': (I, [P]),
+            'lbf_keep_solid_populations': (I, [P]),
             'lbf_initialize_equilibrium': (I, [P, P, U32, U32]),
             'lbf_block_sums': (I, [P, U32, D, ctypes.c_size_t]),
             'lbf_add_density': (I, [P, P]),
@@ -222,6 +223,11 @@ class Engine:
 
     def initialize(self):
         self._ck(self._lib.lbf_initialize(self._h))
+
+    def keep_solid_populations(self):
+        """Carry solid voxels' streamed populations (checkpoints identical to
+        the reference's at solid voxels too); call before initialize."""
+        self._ck(self._lib.lbf_keep_solid_populations(self._h))
 
     def block_sums(self, block, out=None):
         """Per-cube sums of the last written fields, (NBz, NBy, NBx, 5) of

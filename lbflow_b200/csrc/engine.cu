@@ -45,6 +45,9 @@ struct lbf_engine {
     double* partial = nullptr;
     double* dense_tmp = nullptr;    // FP64 copy of reduced-precision populations (dense output)
     double* stage = nullptr;        // device staging of dense outputs bound for host memory
+    double* solid_f[2] = {nullptr, nullptr};   // populations of solid voxels (lbf_keep_solid_populations)
+    int scur = 0;
+    size_t ns = 0;                  // solid voxels (N - nf)
     double* red = nullptr;
     double* h_red = nullptr;        // pinned
     cudaStream_t stream = nullptr;
@@ -219,10 +222,25 @@ Macros macros_of(const lbf_engine* e)
     return m;
 }
 
+unsigned dense_blocks(size_t N);
+template <class L>
+__global__ void solid_stream(const lbf::Grid g, int phases, const double* __restrict__ fin,
+                             const double* __restrict__ sin, double* __restrict__ sout, size_t ns, size_t N);
+
 void launch_step(lbf_engine* e, bool pull, int out)
 {
     const void* fin = e->f[e->cur];
     void* fout = e->f[e->cur ^ 1];
+    if (pull && e->solid_f[0]) {
+        const Grid g = grid_of(e);
+        if (e->D == 3)
+            solid_stream<D3Q19><<<dense_blocks(e->N), 256, 0, e->stream>>>(
+                g, e->phases, static_cast<const double*>(fin), e->solid_f[e->scur], e->solid_f[e->scur ^ 1], e->ns, e->N);
+        else
+            solid_stream<D2Q9><<<dense_blocks(e->N), 256, 0, e->stream>>>(
+                g, e->phases, static_cast<const double*>(fin), e->solid_f[e->scur], e->solid_f[e->scur ^ 1], e->ns, e->N);
+        e->scur ^= 1;
+    }
     if (e->cfg.model == LBF_MODEL_SCSP) {
         // FP16 / BF16 storage rounds stochastically, with a fresh seed every
         // step (deterministic for a given run); the t = 0 collision rounds to
@@ -456,6 +474,60 @@ void set_global_error(const std::string& msg) { g_create_error = msg; }
 }  // namespace lbf
 
 namespace {
+// Populations of solid voxels (checkpoint compatibility).  The reference
+// streams every voxel, fluid or solid (Simulator::streaming,
+// simulator.cpp:73-101), collides only fluid ones, and bounce-back overwrites
+// every population a fluid voxel receives from a solid one
+// (simulator.cpp:103-111), so solid voxels carry values that never reach the
+// fluid but do appear in its checkpoints (scsp.cpp:277-302).  They are kept in
+// their own array [phase][q][solid index]; the solid index of voxel v is v
+// minus the number of fluid voxels before it.  One pull step: a solid voxel's
+// q population comes from x - e_q, the post-collision value of the previous
+// step (fin for a fluid source, the old solid array for a solid one); the
+// rest population is never streamed and stays as initialised (0).
+template <class L>
+__global__ void solid_stream(const lbf::Grid g, int phases, const double* __restrict__ fin,
+                             const double* __restrict__ sin, double* __restrict__ sout, size_t ns, size_t N)
+{
+    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < N; v += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(v % g.nx);
+        const int y = (int)((v / g.nx) % g.ny);
+        const int z = (int)(v / ((size_t)g.nx * g.ny));
+        bool fluid;
+        const uint32_t before = lbf::lookup(g, x, y, z, fluid);
+        if (fluid) continue;
+        const size_t si = v - before;
+        for (int p = 0; p < phases; ++p) {
+            const size_t b0 = (size_t)p * L::Q;
+            sout[b0 * ns + si] = sin[b0 * ns + si];
+#pragma unroll
+            for (int q = 1; q < L::Q; ++q) {
+                const int sx = lbf::wrap(x - L::ex(q), g.nx), sy = lbf::wrap(y - L::ey(q), g.ny);
+                const int sz = L::D == 3 ? lbf::wrap(z - L::ez(q), g.nz) : 0;
+                bool sf;
+                const uint32_t j = lbf::lookup(g, sx, sy, sz, sf);
+                const size_t sv = ((size_t)sz * g.ny + sy) * g.nx + sx;
+                sout[(b0 + q) * ns + si] = sf ? fin[(b0 + q) * g.nfp + j] : sin[(b0 + q) * ns + (sv - j)];
+            }
+        }
+    }
+}
+
+// Solid entries of a dense [block][voxel] array into the solid array.
+__global__ void solid_from_dense(const lbf::Grid g, int blocks, const double* __restrict__ dense,
+                                 double* __restrict__ s, size_t ns, size_t N)
+{
+    for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < N; v += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(v % g.nx);
+        const int y = (int)((v / g.nx) % g.ny);
+        const int z = (int)(v / ((size_t)g.nx * g.ny));
+        bool fluid;
+        const uint32_t before = lbf::lookup(g, x, y, z, fluid);
+        if (fluid) continue;
+        for (int b = 0; b < blocks; ++b) s[(size_t)b * ns + (v - before)] = dense[(size_t)b * N + v];
+    }
+}
+
 // Dense outputs of voxels [v0, v0 + r), one thread per voxel (grid-stride),
 // x fastest, so that a warp writes consecutive addresses of every array.
 // Fields: out = [rho0 r][rho1 r (color)][velocity r x D interleaved];
@@ -483,7 +555,8 @@ __global__ void fields_range_kernel(const lbf::Grid g, const double* __restrict_
 }
 
 __global__ void populations_range_kernel(const lbf::Grid g, const double* __restrict__ in, int blocks, size_t v0,
-                                         size_t r, double* __restrict__ out, uint32_t* __restrict__ err)
+                                         size_t r, double* __restrict__ out, uint32_t* __restrict__ err,
+                                         const double* __restrict__ solid, size_t ns)
 {
     bool bad = false;
     for (size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x; j < r; j += (size_t)gridDim.x * blockDim.x) {
@@ -494,7 +567,7 @@ __global__ void populations_range_kernel(const lbf::Grid g, const double* __rest
         bool fluid;
         const uint32_t k = lbf::lookup(g, x, y, z, fluid);
         for (int b = 0; b < blocks; ++b) {
-            const double val = fluid ? in[(size_t)b * g.nfp + k] : 0.0;
+            const double val = fluid ? in[(size_t)b * g.nfp + k] : (solid ? solid[(size_t)b * ns + (v - k)] : 0.0);
             bad |= !isfinite(val);
             out[(size_t)b * r + j] = val;
         }
@@ -1032,7 +1105,7 @@ void lbf_destroy(lbf_engine* e)
                     e->rho0, e->rho1, e->u, e->uprev, e->uadj, e->ind, e->indprev, e->indadj,
                     e->phi, e->angle_id, e->angles, e->tib, e->err, e->partial, e->red,
                     e->zh_node, e->zh_code, e->zh_value, e->zh_num, e->dense_tmp, e->film_bits[0], e->film_bits[1],
-                    e->stage, e->phid};
+                    e->stage, e->phid, e->solid_f[0], e->solid_f[1]};
     for (void* p : ptrs) if (p) cudaFreeAsync(p, e->stream);
     if (e->stream) cudaStreamSynchronize(e->stream);
     if (e->h_red) cudaFreeHost(e->h_red);
@@ -1040,13 +1113,36 @@ void lbf_destroy(lbf_engine* e)
     delete e;
 }
 
+int lbf_keep_solid_populations(lbf_engine* e)
+{
+    if (!e) return fail(e, LBF_EINVAL, "NULL engine");
+    if (e->cfg.storage != LBF_STORE_FP64)
+        return fail(e, LBF_EINVAL, "solid-voxel populations are kept with FP64 storage only");
+    if (e->solid_f[0]) return LBF_OK;
+    int rc = setdev(e);
+    if (rc) return rc;
+    e->ns = e->N - e->nf;
+    const size_t count = (size_t)e->phases * e->Q * (e->ns ? e->ns : 1);
+    for (int b = 0; b < 2; ++b) {
+        if ((rc = dalloc(e, &e->solid_f[b], count))) return rc;
+        LBF_CK(e, cudaMemsetAsync(e->solid_f[b], 0, count * sizeof(double), e->stream));
+    }
+    e->scur = 0;
+    if ((rc = ensure_vox(e))) return rc;
+    LBF_CK(e, cudaStreamSynchronize(e->stream));
+    return LBF_OK;
+}
+
 int lbf_initialize(lbf_engine* e)
 {
     if (!e) return fail(e, LBF_EINVAL, "NULL engine");
     int rc = setdev(e);
     if (rc) return rc;
-    // A fresh t = 0 state starts with a clear device error word.
+    // A fresh t = 0 state starts with a clear device error word (and solid
+    // voxels at 0, as the reference's initialisation leaves them).
     LBF_CK(e, cudaMemsetAsync(e->err, 0, sizeof(uint32_t), e->stream));
+    if (e->solid_f[0])
+        LBF_CK(e, cudaMemsetAsync(e->solid_f[e->scur], 0, (size_t)e->phases * e->Q * e->ns * sizeof(double), e->stream));
     const Grid g = grid_of(e);
     if (e->cfg.model == LBF_MODEL_SCSP)
         launch_scsp_init(e->D, (int)e->cfg.storage, g, e->force, e->cfg.rho[0], e->f[e->cur], e->ex[e->cur],
@@ -1201,6 +1297,22 @@ int lbf_get_populations(lbf_engine* e, double* host, size_t n)
             double* dst = host + ((size_t)p * e->Q + q) * e->N;
             for (uint32_t k = 0; k < e->nf; ++k) dst[e->vox[k]] = src[k];
         }
+    if (e->solid_f[0]) {
+        // Solid voxels' streamed populations (lbf_keep_solid_populations).
+        const size_t blocks = (size_t)e->phases * e->Q;
+        std::vector<double> sv(blocks * e->ns);
+        if (!sv.empty()) {
+            LBF_CK(e, cudaMemcpyAsync(sv.data(), e->solid_f[e->scur], sv.size() * sizeof(double),
+                                      cudaMemcpyDeviceToHost, e->stream));
+            LBF_CK(e, cudaStreamSynchronize(e->stream));
+        }
+        size_t k = 0, si = 0;
+        for (size_t v = 0; v < e->N; ++v) {
+            if (k < e->nf && e->vox[k] == v) { ++k; continue; }
+            for (size_t b = 0; b < blocks; ++b) host[b * e->N + v] = sv[b * e->ns + si];
+            ++si;
+        }
+    }
     return LBF_OK;
 }
 
@@ -1220,6 +1332,20 @@ int lbf_set_populations(lbf_engine* e, const double* host, size_t n)
             double* dst = compact.data() + ((size_t)p * e->Q + q) * e->nfp;
             for (uint32_t k = 0; k < e->nf; ++k) dst[k] = src[e->vox[k]];
         }
+    if (e->solid_f[0]) {
+        // Solid voxels' values of the checkpoint (scsp.cpp:277-302 writes them).
+        const size_t blocks = (size_t)e->phases * e->Q;
+        std::vector<double> sv(blocks * e->ns);
+        size_t k = 0, si = 0;
+        for (size_t v = 0; v < e->N; ++v) {
+            if (k < e->nf && e->vox[k] == v) { ++k; continue; }
+            for (size_t b = 0; b < blocks; ++b) sv[b * e->ns + si] = host[b * e->N + v];
+            ++si;
+        }
+        if (!sv.empty())
+            LBF_CK(e, cudaMemcpyAsync(e->solid_f[e->scur], sv.data(), sv.size() * sizeof(double),
+                                      cudaMemcpyHostToDevice, e->stream));
+    }
     if (e->cfg.storage == LBF_STORE_FP64) {
         LBF_CK(e, cudaMemcpyAsync(e->f[e->cur], compact.data(), count * sizeof(double), cudaMemcpyHostToDevice, e->stream));
         LBF_CK(e, cudaStreamSynchronize(e->stream));
@@ -1299,7 +1425,8 @@ int lbf_populations_dense_async(lbf_engine* e, double* out, size_t n)
     if (e->N == 0) return LBF_OK;
     const Grid g = grid_of(e);
     if (dst == Dest::kDevice) {
-        populations_range_kernel<<<dense_blocks(e->N), 256, 0, e->stream>>>(g, src, (int)blocks, 0, e->N, out, e->err);
+        populations_range_kernel<<<dense_blocks(e->N), 256, 0, e->stream>>>(g, src, (int)blocks, 0, e->N, out, e->err,
+                                                                            e->solid_f[e->scur], e->ns);
         LBF_CK(e, cudaGetLastError());
         return LBF_OK;
     }
@@ -1308,7 +1435,8 @@ int lbf_populations_dense_async(lbf_engine* e, double* out, size_t n)
     const size_t chunk = kStageBytes / (sizeof(double) * blocks);
     for (size_t v0 = 0; v0 < e->N; v0 += chunk) {
         const size_t r = std::min(chunk, e->N - v0);
-        populations_range_kernel<<<dense_blocks(r), 256, 0, e->stream>>>(g, src, (int)blocks, v0, r, st, e->err);
+        populations_range_kernel<<<dense_blocks(r), 256, 0, e->stream>>>(g, src, (int)blocks, v0, r, st, e->err,
+                                                                         e->solid_f[e->scur], e->ns);
         LBF_CK(e, cudaGetLastError());
         // [block][r] in the stage -> [block][N] at voxel v0 in out.
         LBF_CK(e, cudaMemcpy2DAsync(out + v0, e->N * sizeof(double), st, r * sizeof(double), r * sizeof(double),

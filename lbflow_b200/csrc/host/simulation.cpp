@@ -137,6 +137,13 @@ Simulation::Simulation(const Params& p) : p_(p)
     }
     const int rc = lbf_create(&c, labels.data(), geometry_.data(), &e_);
     if (rc != LBF_OK) throw std::runtime_error(std::string("engine: ") + lbf_last_error(nullptr));
+    // Optional extension key: checkpoints with the reference's values at
+    // solid voxels too (lbf_keep_solid_populations).
+    const std::string solids = p.selector("solidPopulations", "zero", "solidPopulations");
+    if (solids != "zero" && solids != "stream")
+        throw std::invalid_argument("solidPopulations must be zero or stream.");
+    if (solids == "stream" && lbf_keep_solid_populations(e_) != LBF_OK)
+        throw std::runtime_error(std::string("engine: ") + lbf_last_error(e_));
 
     if (p.reportDir() != 0) {
         axis_ = qaxis(D_, p.reportDir());

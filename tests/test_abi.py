@@ -107,3 +107,9 @@ def test_noalloc_rejects_bad_arguments(args, msg):
     rc = lib.lbf_flux_sums_noalloc(a['u'], a['rho0'], None, a['n'], a['stride'], a['out'], None)
     assert rc == -1
     assert msg in lib.lbf_last_error(None).decode()
+
+
+def test_keep_solid_populations_null_engine():
+    import lbflow_b200
+    lib = lbflow_b200.library()
+    assert lib.lbf_keep_solid_populations(None) == -1

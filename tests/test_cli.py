@@ -119,6 +119,20 @@ def test_cli_matches_reference_outputs(tmp_path, case):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize('case', [porous_scsp('MRT'), porous_scsp('SRT')], ids=lambda c: c['name'])
+def test_cli_checkpoint_with_solid_populations(tmp_path, case):
+    """`solidPopulations "stream";`: the checkpoint holds the reference's
+    values at solid voxels too (the whole .rst against the reference's)."""
+    gold = load_golden(case['name'])
+    code, out = run_cli(tmp_path, case, prm=prm_text(case) + 'solidPopulations "stream";\n')
+    assert code == 0 and 'Simulation finished!' in out, out[-2000:]
+    f = np.fromfile(tmp_path / f'field.{case["steps"]:010d}.rst')
+    ref = gold['populations']
+    assert f.shape == ref.shape
+    assert np.max(np.abs(f - ref) / np.maximum(np.abs(ref), 1e-3)) <= 1e-12
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize('case', [channel_mrt(), wall_color_2d('MRT')], ids=lambda c: c['name'])
 def test_vti_header_and_sidecar_bytes(tmp_path, case):
     code, out = run_cli(tmp_path, case)

@@ -212,3 +212,45 @@ def test_mass_conservation_and_determinism():
             runs.append(e.populations())
         assert abs(m1 - m0) / m0 < 1e-13
     assert np.array_equal(runs[0], runs[1])
+
+
+SOLID_CASES = [c for c in CASES if c['name'] in (
+    'channel-mrt', 'porous-scsp-MRT', 'porous-scsp-SRT', 'porous-scsp-2d-MRT',
+    'wall-color-3d-MRT-0.7', 'pb-porous-d3-MRT', 'entry-h16-ratio1.5-MRT', 'film-d3-MRT')]
+
+
+@pytest.mark.parametrize('case', SOLID_CASES, ids=[c['name'] for c in SOLID_CASES])
+def test_checkpoint_with_solid_populations_matches_reference(case):
+    """lbf_keep_solid_populations: the whole population array, solid voxels
+    included (the reference streams through them), against the reference's
+    own checkpoint, at the same tolerance as the fluid voxels."""
+    gold = load_golden(case['name'])
+    with engine_for(case) as e:
+        e.keep_solid_populations()
+        e.initialize()
+        e.step(case['steps'], macros=True)
+        e.check()
+        f = e.populations()
+    ref = gold['populations'].reshape(f.shape)
+    everywhere = np.ones(f.shape[2:], bool)
+    solid = ~fluid_mask(case)
+    solid = solid if solid.ndim == 3 else solid[None]
+    assert np.any(ref[:, :, solid] != 0), 'the case has no streamed solid values'
+    assert_populations_close(f, ref, everywhere, population_tolerance(case, case['steps']))
+
+
+def test_solid_populations_survive_a_restart():
+    """A checkpoint written with solid populations and loaded again continues
+    exactly (loadRst semantics, solid voxels included)."""
+    case = CASES[7]
+    o = Oracle(case)
+    o.start()
+    o.step(20)
+    mid = o.populations()
+    o.step(15)
+    with engine_for(case) as e:
+        e.keep_solid_populations()
+        e.set_populations(mid)
+        e.step(15, macros=True)
+        f = e.populations()
+    assert_populations_close(f, o.populations(), np.ones(f.shape[2:], bool))
