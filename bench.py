@@ -293,7 +293,9 @@ def main():
     ap.add_argument('--max-steps', type=int, default=400000)
     ap.add_argument('--io-write', type=int, default=500, help='io: VTI write interval')
     ap.add_argument('--io-restart', type=int, default=1000, help='io: checkpoint interval')
-    ap.add_argument('--workload', default='scsp', choices=('scsp', 'color', 'batch', 'operator', 'io'),
+    ap.add_argument('--color-steps', type=int, default=50000, help='color-precision: steps of each run')
+    ap.add_argument('--workload', default='scsp', choices=('scsp', 'color', 'color-precision', 'batch', 'operator',
+                                                           'io'),
                     help='scsp: 256^3 single-phase cube; color: 128x128x256 two-phase color-gradient MRT; '
                          'batch: many uneven geometries in one launch; operator: the warm-start network '
                          '(forward + backward) on the tensor cores; io: output cost of a command-line run')
@@ -334,6 +336,8 @@ def main():
         return time_to_permeability(args)
     if args.workload == 'color':
         return color_throughput(args)
+    if args.workload == 'color-precision':
+        return color_precision(args)
     if args.workload == 'batch':
         return batch_run(args)
     if args.workload == 'operator':
@@ -480,6 +484,47 @@ def color_throughput(args):
                                         unit='GB/s', bytes_per_node=alg, peak_kind=kind),
                           saturation_phase0=sums[8] / nf, clocks=clocks.summary())))
     eng.close()
+    return 0
+
+
+def color_precision(args):
+    """The two-phase workload run to --color-steps (default 50,000) with FP64,
+    FP32, FP16 and BF16 storage: phase-0 saturation, phase-0 mass drift over
+    the run and the phase-fraction-weighted Darcy flux of each phase along the
+    force (scripts/porous_media.py:20-44: means of phi_k u over all voxels),
+    each storage's error against FP64, and the wall time."""
+    import torch
+    from lbflow_b200 import Engine
+    torch.cuda.set_device(0)
+    g, labels = color_geometry()
+    N = g.size
+    out = {}
+    for storage in ('fp64', 'fp32', 'fp16', 'bf16'):
+        with Engine(g, labels, model='color', collision=args.collision, tau=(1.0, 0.7), rho=(1.0, 1.0),
+                    alpha0=1 / 3, sigma=1e-3, beta=0.7, storage=storage) as eng:
+            eng.initialize()
+            s0 = eng.flux_sums()
+            eng.synchronize()
+            t0 = time.perf_counter()
+            eng.step(args.color_steps, macros=True)
+            eng.synchronize()
+            sec = time.perf_counter() - t0
+            eng.check()
+            s1 = eng.flux_sums()
+            nf = eng.fluid_nodes
+        out[storage] = dict(saturation_phase0=s1[8] / nf, mass_drift_phase0=(s1[6] - s0[6]) / s0[6],
+                            mass_drift_phase1=(s1[7] - s0[7]) / s0[7],
+                            darcy_flux_z=s1[2] / N, phase_flux_z=[s1[5] / N, (s1[2] - s1[5]) / N],
+                            seconds=sec, mlups=nf * args.color_steps / sec / 1e6)
+    ref = out['fp64']
+    for k, v in out.items():
+        v['saturation_rel_error'] = abs(v['saturation_phase0'] - ref['saturation_phase0']) / ref['saturation_phase0']
+        v['darcy_flux_rel_error'] = abs(v['darcy_flux_z'] - ref['darcy_flux_z']) / abs(ref['darcy_flux_z'])
+        v['phase_flux_rel_error'] = [abs(a - b) / abs(b) for a, b in zip(v['phase_flux_z'], ref['phase_flux_z'])]
+    print(json.dumps(dict(metric='two-phase workload, reduced-precision storage against FP64',
+                          workload='128x128x256 color-gradient MRT, sigma 2, porosity 0.30, inlet third phase A, '
+                                   'tau 1/0.7, A 1e-3, beta 0.7, 60-degree walls, g_z 2e-6',
+                          steps=args.color_steps, runs=out)))
     return 0
 
 
