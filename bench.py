@@ -932,7 +932,11 @@ def end_to_end(geometry, args, device, repeats=3):
     import torch
     fields = HostBuffer(4 * geometry.size)
     fields.array[::512] = 0.0          # touch the pages before timing
-    geom = np.ascontiguousarray(geometry)
+    # The step's input (the voxel labels) in page-locked memory, as the
+    # caller of a production run holds it.
+    gbuf = HostBuffer(geometry.size, dtype=np.uint8)
+    geom = gbuf.array.reshape(geometry.shape)
+    geom[...] = geometry
     runs = []
     for _ in range(repeats):
         torch.cuda.synchronize()
@@ -957,6 +961,8 @@ def end_to_end(geometry, args, device, repeats=3):
             raise RuntimeError('end-to-end run produced non-finite output')
         runs.append(dict(seconds=t3 - t, create=t1 - t, steps=t2 - t1, fields=t3 - t2))
     fields.close()
+    del geom
+    gbuf.close()
     runs.sort(key=lambda r: r['seconds'])
     med = runs[len(runs) // 2]
     h2d = geometry.nbytes + 256 * 24

@@ -125,18 +125,20 @@ def make_labels(labels):
 
 
 class HostBuffer:
-    """Page-locked host memory the device can write (lbf_host_alloc), viewed
-    as a float64 numpy array; the destination of the engine's *_dense_async
-    outputs."""
+    """Page-locked host memory the device can read and write (lbf_host_alloc),
+    viewed as a numpy array (float64 by default): the destination of the
+    engine's *_dense_async outputs, or a geometry to upload by DMA."""
 
-    def __init__(self, count):
+    def __init__(self, count, dtype=np.float64):
         self._lib = library()
         self.ptr = ctypes.c_void_p()
-        rc = self._lib.lbf_host_alloc(int(count) * 8, ctypes.byref(self.ptr))
+        dtype = np.dtype(dtype)
+        rc = self._lib.lbf_host_alloc(int(count) * dtype.itemsize, ctypes.byref(self.ptr))
         if rc != 0:
             raise LbfError(rc, self._lib.lbf_last_error(None).decode())
         self.count = int(count)
-        self.array = np.ctypeslib.as_array((ctypes.c_double * self.count).from_address(self.ptr.value))
+        raw = (ctypes.c_uint8 * (self.count * dtype.itemsize)).from_address(self.ptr.value)
+        self.array = np.frombuffer(raw, dtype=dtype, count=self.count)
 
     def close(self):
         if self.ptr:
@@ -179,7 +181,10 @@ class Engine:
                       (ctypes.c_double * 2)(*tau), (ctypes.c_double * 2)(*rho), alpha0, sigma, beta)
         self._labels = make_labels(labels)
         h = ctypes.c_void_p()
-        rc = self._lib.lbf_create(ctypes.byref(cfg), self._labels, g.tobytes(), ctypes.byref(h))
+        # The library reads the N label bytes during the call: pass the
+        # array's own buffer (page-locked if the caller allocated it so).
+        rc = self._lib.lbf_create(ctypes.byref(cfg), self._labels, ctypes.cast(g.ctypes.data, ctypes.c_char_p),
+                                  ctypes.byref(h))
         if rc != 0:
             raise LbfError(rc, self._lib.lbf_last_error(None).decode())
         self._h = h
