@@ -321,6 +321,7 @@ def main():
     ap.add_argument('--check', type=int, default=8, help='batch: geometries re-solved alone in FP64')
     ap.add_argument('--ref-steps', type=int, default=3, help='reference arm: steps per reference process')
     ap.add_argument('--no-ttp', action='store_true', help='default line without the time-to-permeability runs')
+    ap.add_argument('--no-others', action='store_true', help='default line without the other workloads\' rates')
     ap.add_argument('--cap16', type=int, default=0, help='ttp: step cap of 16-bit runs (0: --max-steps)')
     ap.add_argument('--ttp-runs', default='fp64,fp16+acc,fp16+mob',
                     help='runs of the default line\'s time-to-permeability object')
@@ -409,6 +410,9 @@ def main():
     ttp = None
     if rank == 0 and world == 1 and not args.no_ttp and args.storage == 'fp64' and args.size % 8 == 0:
         ttp = ttp_line(args)
+    others = None
+    if rank == 0 and world == 1 and not args.no_others and args.storage == 'fp64':
+        others = other_workloads(args, geometry)
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -430,7 +434,7 @@ def main():
                                   frac=achieved / peak, traffic=traffic, peak_kind=peak_kind,
                                   bytes_per_launch=bytes_launch, launch_ms=launch_ms),
                     gpu_launches=args.steps,
-                    clocks=clk, e2e=e2e, cpu_baseline=base, ttp=ttp)
+                    clocks=clk, e2e=e2e, cpu_baseline=base, ttp=ttp, workloads=others)
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
@@ -817,6 +821,72 @@ def time_to_permeability(args):
                           workload=f'D3Q19 {args.collision}, tau 1, g_x 1e-5, periodic porous media',
                           summary=summary)))
     return 0
+
+
+def _timed_steps(stream, run, steps):
+    """CUDA-event milliseconds of run() (which enqueues `steps` steps) on `stream`."""
+    import torch
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0.record(stream)
+    run()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    return t0.elapsed_time(t1)
+
+
+def other_workloads(args, geometry):
+    """Sub-objects of the default line for the other workloads, each device-
+    timed with CUDA events after warm-up steps: the 256^3 cube with FP32 and
+    FP16 storage, the two-phase 128x128x256 medium (FP64 and FP16 storage)
+    and 64 uneven media in one batched launch (FP64)."""
+    import torch
+    from lbflow_b200 import Engine
+    from lbflow_b200.batch import Batch
+    peak, kind = measured_peaks()
+    out = {}
+    for storage in ('fp32', 'fp16'):
+        with Engine(geometry, LABELS, model='scsp', collision=args.collision, tau=(1.0,), rho=(1.0,),
+                    storage=storage) as e:
+            e.initialize()
+            e.step(args.warmup)
+            steps = 40
+            ms = _timed_steps(torch.cuda.ExternalStream(e.stream), lambda: e.step(steps), steps)
+            e.check()
+            nf = e.fluid_nodes
+        b = ALG_BYTES[storage]
+        out[f'scsp_{storage}'] = dict(value=nf * steps / (ms / 1e3) / 1e6, unit='MLUPS', ms_per_step=ms / steps,
+                                      bytes_per_node=b, frac=nf * b * steps / (ms / 1e3) / 1e9 / peak)
+    g, labels = color_geometry()
+    for storage in ('fp64', 'fp16'):
+        with Engine(g, labels, model='color', collision=args.collision, tau=(1.0, 0.7), rho=(1.0, 1.0),
+                    alpha0=1 / 3, sigma=1e-3, beta=0.7, storage=storage) as e:
+            e.initialize()
+            e.step(args.warmup)
+            steps = 40
+            ms = _timed_steps(torch.cuda.ExternalStream(e.stream), lambda: e.step(steps), steps)
+            e.check()
+            nf = e.fluid_nodes
+        b = 2 * (2 * 19 * ELEM[storage]) + 2 * 8 + 4
+        out[f'color_{storage}'] = dict(value=nf * steps / (ms / 1e3) / 1e6, unit='MLUPS', ms_per_step=ms / steps,
+                                       bytes_per_node=b, frac=nf * b * steps / (ms / 1e3) / 1e9 / peak,
+                                       workload='128x128x256 two-phase color MRT, sigma 2, porosity 0.30')
+    geoms, taus, _ = batch_geometries(64)
+    with Batch(geoms, taus, LABELS, collision=args.collision, storage='fp64') as bt:
+        bt.initialize()
+        tune = bt.autotune(steps=6)
+        bt.step(64)
+        steps = 640
+        ms = _timed_steps(torch.cuda.ExternalStream(bt.stream), lambda: bt.step(steps), steps)
+        bt.check()
+        nf = bt.fluid_nodes()
+    out['batch_fp64'] = dict(value=nf * steps / (ms / 1e3) / 1e6, unit='MLUPS', ms_per_step=ms / steps,
+                             bytes_per_node=308, frac=nf * 308 * steps / (ms / 1e3) / 1e9 / peak,
+                             workload='64 uneven media (edges 32-128, porosity 0.10-0.35) in one launch',
+                             fluid_nodes=int(nf), autotune=tune)
+    out['peak_gbs'] = peak
+    out['peak_kind'] = kind
+    return out
 
 
 def ttp_line(args):
