@@ -989,7 +989,7 @@ def operator_run(args):
                           gpu_launches=None, clocks=clocks)))
     return 0
 
-def end_to_end(geometry, args, device, repeats=3):
+def end_to_end(geometry, args, device, repeats=5):
     """Same metric through the C ABI with host buffers: the uint8 geometry
     from the host (classified on the device), initialization, K steps each
     followed by the read-back of the step's flux and mass sums (the numbers
