@@ -15,14 +15,18 @@
 //         (channels contiguous), the long reduction over rows split across
 //         CTAs with fixed-order partial sums.  Weight gradients run here.
 //
-// Block: 128 threads = one warpgroup; every thread gathers 16-byte pieces
-// with cp.async into a 3-stage ring of 128-byte-swizzled operand tiles,
-// thread 0 issues four M=128 x N x K=16 MMAs per 64-wide K stage and commits
-// them to the stage's mbarrier; the ring slot is refilled once that barrier
-// fires.  The epilogue reads the accumulator rows back with tcgen05.ld (warp
-// w owns TMEM lanes 32w..32w+31 = tile rows).  Every wait is bounded: on
-// timeout the kernel sets LBF_ERR_MMA_TIMEOUT, stops issuing and still
-// releases its tensor memory.
+// Block: 160 threads, warp-specialised.  Warps 0-3 (128 producer threads)
+// gather 16-byte pieces with cp.async into a 3-stage ring of
+// 128-byte-swizzled operand tiles; each producer's copies of a stage arrive
+// on the stage's `full` mbarrier (cp.async.mbarrier.arrive, 128 arrivals), so
+// no producer waits for its own loads.  One thread of warp 4 waits for
+// `full`, issues four M=128 x N x K=16 MMAs per 64-wide K stage and commits
+// them to the stage's `empty` mbarrier, which the producers wait on before
+// refilling the slot; its last commit arrives on `done`.  The epilogue (warps
+// 0-3) reads the accumulator rows back with tcgen05.ld (warp w owns TMEM
+// lanes 32w..32w+31 = tile rows).  Every wait is bounded: on timeout the
+// kernel sets LBF_ERR_MMA_TIMEOUT, stops issuing and still releases its
+// tensor memory.
 #include "../../include/lbflow.h"
 #include "../../include/lbflow_operator.h"
 #include "internal.h"
@@ -38,7 +42,8 @@ namespace {
 
 using namespace lbf::umma;
 
-constexpr int kThreads = 128;
+constexpr int kProducers = 128;        // warps 0-3: operand gathers, then the epilogue
+constexpr int kThreads = kProducers + 32;   // + warp 4: the MMA issuer
 constexpr int kBM = 128;             // tile rows = UMMA M
 constexpr int kBK = 64;              // K per stage: one 128-byte swizzle row of bf16
 constexpr int kStages = 3;
@@ -90,10 +95,11 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
 }
 
 struct SmemRing {
-    uint32_t a0, b0, b_bytes, mbar0, tmem_slot;
+    uint32_t a0, b0, b_bytes, full0, empty0, done, tmem_slot;
     __device__ uint32_t a(int s) const { return a0 + uint32_t(s) * kTileA; }
     __device__ uint32_t b(int s) const { return b0 + uint32_t(s) * b_bytes; }
-    __device__ uint32_t mbar(int s) const { return mbar0 + uint32_t(s) * 8u; }
+    __device__ uint32_t full(int s) const { return full0 + uint32_t(s) * 8u; }
+    __device__ uint32_t empty(int s) const { return empty0 + uint32_t(s) * 8u; }
 };
 
 __device__ __forceinline__ SmemRing carve(uint8_t* raw, uint32_t b_bytes) {
@@ -102,13 +108,15 @@ __device__ __forceinline__ SmemRing carve(uint8_t* raw, uint32_t b_bytes) {
     r.a0 = base;
     r.b0 = base + kStages * kTileA;
     r.b_bytes = b_bytes;
-    r.mbar0 = r.b0 + kStages * b_bytes;
-    r.tmem_slot = r.mbar0 + kStages * 8u;
+    r.full0 = r.b0 + kStages * b_bytes;
+    r.empty0 = r.full0 + kStages * 8u;
+    r.done = r.empty0 + kStages * 8u;
+    r.tmem_slot = r.done + 8u;
     return r;
 }
 
 constexpr size_t smem_bytes(uint32_t b_bytes) {
-    return 1024 + kStages * (kTileA + b_bytes) + kStages * 8 + 16;
+    return 1024 + kStages * (kTileA + b_bytes) + (2 * kStages + 1) * 8 + 16;
 }
 
 // Allocation of `cols` TMEM columns by warp 0 and the barrier set-up.
@@ -118,7 +126,11 @@ __device__ __forceinline__ uint32_t prologue(const SmemRing& r, uint32_t cols) {
         tmem_relinquish();
     }
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kStages; ++s) mbar_init(r.mbar(s), 1);
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(r.full(s), kProducers);
+            mbar_init(r.empty(s), 1);
+        }
+        mbar_init(r.done, 1);
         mbar_init_fence();
     }
     fence_before_sync();
@@ -135,47 +147,54 @@ __device__ __forceinline__ void release(uint32_t tmem, uint32_t cols) {
     if (threadIdx.x < 32) tmem_dealloc(tmem, cols);
 }
 
-// The shared producer/MMA loop.  Loader provides
+// The shared producer / MMA pipeline.  Loader provides (producer threads)
 //   load(chunk, stage)   cp.async the chunk's A and B tiles into the stage
 //   adesc/bdesc(stage, kk)  descriptors of the kk-th K=16 slice
-// Returns false if a wait timed out.
+// Returns, in the producer threads, whether the accumulator is complete
+// (every wait succeeded and `done` fired); false elsewhere or on a timeout.
 template <class Loader>
 __device__ bool mainloop(Loader& ld, const SmemRing& r, uint32_t nch, uint32_t tmem, uint32_t idesc) {
-    bool ok = true;
-#pragma unroll
-    for (int s = 0; s < kStages - 1; ++s) {
-        if (uint32_t(s) < nch) ld.load(uint32_t(s), s);
-        cp_async_commit();
+    const uint32_t warp = threadIdx.x >> 5;
+    if (warp < uint32_t(kProducers / 32)) {
+        bool ok = true;
+        for (uint32_t c = 0; c < nch; ++c) {
+            const int s = int(c % kStages);
+            if (c >= uint32_t(kStages)) {
+                // The slot's previous chunk must have been consumed by its MMAs.
+                const bool w = mbar_wait(r.empty(s), ((c / kStages) - 1u) & 1u, kWaitCycles);
+                ok = __all_sync(0xffffffffu, w);      // the warp leaves together (loads shuffle)
+                if (!ok) break;
+            }
+            ld.load(c, s);
+            cp_async_arrive(r.full(s));
+        }
+        cp_async_commit();          // wait_group only waits for committed copies
+        cp_async_wait<0>();
+        const bool d = mbar_wait(r.done, 0u, kWaitCycles);
+        fence_after_sync();
+        return ok && d;
     }
-    for (uint32_t c = 0; c < nch; ++c) {
-        const int s = int(c % kStages);
-        cp_async_wait<kStages - 2>();
-        fence_async_shared();
-        __syncthreads();
-        if (threadIdx.x == 0 && ok) {
+    if (threadIdx.x == uint32_t(kProducers)) {
+        bool ok = true;
+        for (uint32_t c = 0; c < nch; ++c) {
+            const int s = int(c % kStages);
+            ok = mbar_wait(r.full(s), (c / kStages) & 1u, kWaitCycles);
+            if (!ok) break;
+            // The producers' cp.async writes, made visible to the tensor
+            // core's (async-proxy) reads of the stage.
+            fence_async_shared();
             fence_after_sync();
 #pragma unroll
             for (int kk = 0; kk < kBK / 16; ++kk)
                 mma_bf16(tmem, ld.adesc(s, kk), ld.bdesc(s, kk), idesc, (c | uint32_t(kk)) != 0u);
-            commit(r.mbar(s));
+            commit(r.empty(s));
         }
-        const uint32_t nc = c + kStages - 1;
-        if (nc < nch) {
-            if (c >= 1 && ok) {
-                const uint32_t pc = c - 1;
-                ok = mbar_wait(r.mbar(int(pc % kStages)), (pc / kStages) & 1u, kWaitCycles);
-            }
-            if (ok) ld.load(nc, int(nc % kStages));
-        }
-        cp_async_commit();
+        // `done` fires once every MMA issued above has completed (at once
+        // when none was issued), also after a timeout, so the tensor memory
+        // is never released under a running MMA.
+        commit(r.done);
     }
-    cp_async_wait<0>();
-    if (nch > 0 && ok) {
-        const uint32_t pc = nch - 1;
-        ok = mbar_wait(r.mbar(int(pc % kStages)), (pc / kStages) & 1u, kWaitCycles);
-    }
-    fence_after_sync();
-    return ok;
+    return false;
 }
 
 // ---------------------------------------------------------------- igemm ----
@@ -297,9 +316,13 @@ __global__ void __launch_bounds__(kThreads, 1) igemm_kernel(const __grid_constan
 
     IgemmLoader<BN> ld(p, r, m0, n0);
     const bool ok = mainloop(ld, r, p.k_pad / kBK, tmem, idesc_bf16(kBM, BN, false, false));
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp >= uint32_t(kProducers / 32)) {
+        release(tmem, kCols);
+        return;
+    }
     if (!ok && threadIdx.x == 0) atomicOr(p.err, LBF_ERR_MMA_TIMEOUT);
 
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t row = m0 + warp * 32 + lane;
     const bool rvalid = ok && row < p.g.rows;
     Coord rc = row_coord(p.g, rvalid ? row : 0u);
@@ -483,7 +506,7 @@ struct WgradLoader {
         }
         // B: BN/8 pieces per K row.
         constexpr uint32_t kPieces = BN / 8;
-        constexpr uint32_t kRowsPerPass = kThreads / kPieces;
+        constexpr uint32_t kRowsPerPass = kProducers / kPieces;
         constexpr uint32_t kSbo = (BN / 64) * 1024u;
         const uint32_t qn = t % kPieces;
         const uint32_t jn = j0 + qn * 8u;
@@ -517,10 +540,15 @@ __global__ void __launch_bounds__(kThreads, 1) wgrad_kernel(const __grid_constan
     const uint32_t m_end = min(p.g.rows, c_end * kBK);
 
     WgradLoader<BN> ld(p, r, i0, j0, c_begin, m_end, st);
-    const bool ok = mainloop(ld, r, c_end > c_begin ? c_end - c_begin : 0u, tmem, idesc_bf16(kBM, BN, true, true));
-    if (!ok && threadIdx.x == 0) atomicOr(p.err, LBF_ERR_MMA_TIMEOUT);
-
+    const uint32_t nch = c_end > c_begin ? c_end - c_begin : 0u;
+    const bool ok = mainloop(ld, r, nch, tmem, idesc_bf16(kBM, BN, true, true));
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp >= uint32_t(kProducers / 32)) {
+        release(tmem, BN);
+        return;
+    }
+    if (!ok && nch > 0 && threadIdx.x == 0) atomicOr(p.err, LBF_ERR_MMA_TIMEOUT);
+
     const uint32_t i = i0 + warp * 32 + lane;
     float* out = p.partial + (size_t(blockIdx.z) * p.mtot + i) * p.cb;
 #pragma unroll 1

@@ -122,6 +122,16 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, long l
     return true;
 }
 
+// Arrive on an mbarrier (counts as one of its expected arrivals).
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(mbar) : "memory");
+}
+// One expected arrival on the mbarrier, made once every cp.async this thread
+// has issued so far has landed in shared memory.
+__device__ __forceinline__ void cp_async_arrive(uint32_t mbar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" :: "r"(mbar) : "memory");
+}
+
 // 16-byte asynchronous global -> shared copy; src_bytes = 0 writes zeros.
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" :: "r"(dst), "l"(src), "r"(src_bytes) : "memory");
