@@ -16,7 +16,7 @@
 //         CTAs with fixed-order partial sums.  Weight gradients run here.
 //
 // Block: 160 threads, warp-specialised.  Warps 0-3 (128 producer threads)
-// gather 16-byte pieces with cp.async into a 3-stage ring of
+// gather 16-byte pieces with cp.async into a 2-stage ring of
 // 128-byte-swizzled operand tiles; each producer's copies of a stage arrive
 // on the stage's `full` mbarrier (cp.async.mbarrier.arrive, 128 arrivals), so
 // no producer waits for its own loads.  One thread of warp 4 waits for
@@ -46,7 +46,11 @@ constexpr int kProducers = 128;        // warps 0-3: operand gathers, then the e
 constexpr int kThreads = kProducers + 32;   // + warp 4: the MMA issuer
 constexpr int kBM = 128;             // tile rows = UMMA M
 constexpr int kBK = 64;              // K per stage: one 128-byte swizzle row of bf16
-constexpr int kStages = 3;
+// Two stages: with the producers decoupled from the MMA issue, the number of
+// CTAs an SM holds (set by shared memory: 4 at 49 KB each) matters more than
+// the ring depth (measured on the heaviest launch: 2 stages 390 TFLOP/s,
+// 3 stages 348, 4 stages 282, 5 stages 177).
+constexpr int kStages = 2;
 constexpr uint32_t kTileA = kBM * kBK * 2;
 constexpr long long kWaitCycles = 4000000000LL;   // about 2 s at the boost clock
 
