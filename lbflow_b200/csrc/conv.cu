@@ -241,6 +241,12 @@ struct IgemmLoader {
     uint32_t n0;
     uint32_t sw;          // swizzle of the thread's row (row mod 8)
     uint32_t poff_b;      // swizzled byte offset of the thread's B piece
+    // Uniform path: the K position of the next chunk (chunks come in order)
+    // as tap (dz, dy, dx) and channel, advanced incrementally instead of by
+    // divisions, and the row's unwrapped source origin stride * voxel - pad.
+    uint32_t u_tap, u_ch;
+    int u_dz, u_dy, u_dx;
+    int oz, oy, ox;
 
     __device__ IgemmLoader(const IgemmArgs& a, const SmemRing& ring, uint32_t m0, uint32_t n0_)
         : p(a), r(ring), n0(n0_) {
@@ -251,24 +257,39 @@ struct IgemmLoader {
         sw = t & 7u;
         poff_b = (((t & 7u) ^ ((t >> 3) & 7u)) << 4);
         uniform = (p.g.ct % kBK == 0) && (p.g.c1 == 0 || p.g.c0 % kBK == 0);
+        u_tap = 0; u_ch = 0;
+        u_dz = u_dy = u_dx = 0;
+        oz = int(p.g.stride) * rc.z - p.g.pad;
+        oy = int(p.g.stride) * rc.y - p.g.pad;
+        ox = int(p.g.stride) * rc.x - p.g.pad;
     }
 
     __device__ void load(uint32_t chunk, int s) {
         const uint32_t t = threadIdx.x;
         const uint32_t a = r.a(s) + t * 128u;
-        uint32_t k = chunk * kBK;
-        uint32_t tap = k / p.g.ct;
-        uint32_t ch = k - tap * p.g.ct;
         if (uniform) {
             // Each thread finds its row's 128 contiguous bytes; the copies are
             // then spread so that lanes 8q..8q+7 move the 8 pieces of one row
-            // (coalesced), the row addresses passed by warp shuffles.
-            const bool v = rv && tap < p.g.taps;
-            const uint16_t* src = p.g.src0;
+            // (coalesced), the row addresses passed by warp shuffles (a null
+            // address marks a row past the end or a K position past the taps).
+            const bool v = rv && u_tap < p.g.taps;
+            const uint16_t* src = nullptr;
             if (v) {
-                int dz, dy, dx;
-                tap_offsets(p.g, tap, dz, dy, dx);
-                src = chan_ptr(p.g, gather_vox(p.g, rc, dz, dy, dx), ch);
+                const int z = wrap(oz + u_dz, int(p.g.in_d));
+                const int y = wrap(oy + u_dy, int(p.g.in_h));
+                const int x = wrap(ox + u_dx, int(p.g.in_w));
+                const size_t vox = ((size_t(rc.b) * p.g.in_d + z) * p.g.in_h + y) * p.g.in_w + x;
+                src = chan_ptr(p.g, vox, u_ch);
+            }
+            // Next chunk: 64 channels further, carrying into the next tap.
+            u_ch += kBK;
+            if (u_ch >= p.g.ct) {
+                u_ch = 0;
+                ++u_tap;
+                if (++u_dx == int(p.g.ks)) {
+                    u_dx = 0;
+                    if (++u_dy == int(p.g.ks)) { u_dy = 0; ++u_dz; }
+                }
             }
             const uint32_t lane = t & 31u, wbase = t & ~31u, j = lane & 7u;
             const unsigned long long sp = reinterpret_cast<unsigned long long>(src);
@@ -276,12 +297,14 @@ struct IgemmLoader {
             for (uint32_t i = 0; i < 8; ++i) {
                 const uint32_t rw = 4u * i + (lane >> 3);              // row within the warp
                 const unsigned long long q = __shfl_sync(0xffffffffu, sp, int(rw));
-                const int vq = __shfl_sync(0xffffffffu, int(v), int(rw));
                 const uint32_t row = wbase + rw;
                 const uint32_t dst = r.a(s) + row * 128u + ((j ^ (row & 7u)) << 4);
-                cp_async16(dst, vq ? reinterpret_cast<const uint16_t*>(q) + 8u * j : p.g.src0, vq ? 16u : 0u);
+                cp_async16(dst, q ? reinterpret_cast<const uint16_t*>(q) + 8u * j : p.g.src0, q ? 16u : 0u);
             }
         } else {
+            uint32_t k = chunk * kBK;
+            uint32_t tap = k / p.g.ct;
+            uint32_t ch = k - tap * p.g.ct;
             uint32_t cur = 0xffffffffu;
             size_t vox = 0;
 #pragma unroll
