@@ -444,8 +444,13 @@ __device__ __forceinline__ void scsp_update(const Grid& g, const Force& F, const
     }
 }
 
+// At most 72 registers per thread (seven 128-thread blocks per SM): the FP64
+// step is latency-bound on the dependent occupancy -> population gather, and
+// 28 warps per SM hide more of it than 16 at the 126 registers it takes
+// unbounded (measured on the 256^3 cube: 18,100 -> 19,270 fluid MLUPS; 32
+// bytes of spill; 8 blocks spill 252 bytes and fall to 12,800).
 template <class L, class S, bool PULL>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 7)
 scsp_step(const Grid g, const Force F, const ScspParams P,
           const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
           Macros mo, const int out, uint32_t* __restrict__ err,
