@@ -444,13 +444,19 @@ __device__ __forceinline__ void scsp_update(const Grid& g, const Force& F, const
     }
 }
 
-// At most 72 registers per thread (seven 128-thread blocks per SM): the FP64
-// step is latency-bound on the dependent occupancy -> population gather, and
-// 28 warps per SM hide more of it than 16 at the 126 registers it takes
-// unbounded (measured on the 256^3 cube: 18,100 -> 19,270 fluid MLUPS; 32
-// bytes of spill; 8 blocks spill 252 bytes and fall to 12,800).
+// Resident 128-thread blocks per SM the step kernel is compiled for.  FP64:
+// seven (at most 72 registers per thread); the step is latency-bound on the
+// dependent occupancy -> population gather, and 28 warps per SM hide more of
+// it than 16 at the 126 registers it takes unbounded (256^3 cube: 18,100 ->
+// 19,270 fluid MLUPS with 32 bytes of spill; eight blocks spill 252 bytes and
+// fall to 12,800).  FP32 arithmetic (the reduced-precision storages): nine
+// (56 registers, no spill); capped at seven they take 72 registers and run
+// slower (FP32 storage 28,650 -> 26,600, FP16 25,050 -> 24,700).
+template <class S> struct StepBlocks { static constexpr int value = 9; };
+template <> struct StepBlocks<StoreF64> { static constexpr int value = 7; };
+
 template <class L, class S, bool PULL>
-__global__ void __launch_bounds__(128, 7)
+__global__ void __launch_bounds__(128, StepBlocks<S>::value)
 scsp_step(const Grid g, const Force F, const ScspParams P,
           const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
           Macros mo, const int out, uint32_t* __restrict__ err,
