@@ -2,11 +2,13 @@
 //
 // A step needs the phase field phi = (rho0 - rho1)/rho of every neighbour
 // after streaming, so it runs as two launches over the fluid nodes:
-//   pass 1  color_phase:   pull both components (with bounce-back), write phi
-//                          (compact and as a dense per-voxel copy);
+//   pass 1  color_phase:   pull both components (with bounce-back), write the
+//                          two component densities (compact) and phi (dense,
+//                          per voxel);
 //   pass 2  color_collide: color gradient from the dense phi (legacy interior
-//           stencil or the geometric wall rotation), pull again, macros,
-//           collision of the total distribution, perturbation and recoloring.
+//           stencil or the geometric wall rotation), pull again into the
+//           total distribution, macros, collision of the total,
+//           perturbation and recoloring.
 // Solid voxels read as phi = 86 (SOLID_DENS_N, colorfluid.cpp:49).
 #pragma once
 #include <type_traits>
@@ -117,6 +119,49 @@ __device__ __forceinline__ uint32_t film_sources(const Grid& g, const uint32_t* 
     return m;
 }
 
+// Both components' incoming populations of node i, handed to sink(q, f0_q,
+// f1_q, source) with source the compact index of the pull source x - e_q, or
+// UINT32_MAX when it is solid (bounce-back).  One neighbour lookup serves both
+// components (the sources are the same).
+template <class L, class S, bool PULL, class Sink>
+__device__ __forceinline__ void color_pull(const Grid& g, const typename S::T* __restrict__ fin, uint32_t i,
+                                           int x, int y, int z, typename S::R rho_bar, Sink&& sink)
+{
+    using R = typename S::R;
+    const typename S::T* __restrict__ fin1 = fin + (size_t)L::Q * g.nfp;
+    const uint32_t nfp = g.nfp;
+    const uint32_t nblk = (uint32_t)L::Q * nfp;
+    auto load2 = [&](uint32_t off, int q, R& a, R& b) {
+        if constexpr (IsPacked<S>::value) S::load_pair(fin, off, nblk, q, rho_bar, a, b);
+        else { a = S::load(fin + off, q, R(0)); b = S::load(fin1 + off, q, R(0)); }
+    };
+    {
+        R a, b;
+        load2(i, 0, a, b);
+        sink(0, a, b, i);
+    }
+    if constexpr (!PULL) {
+#pragma unroll
+        for (int q = 1; q < L::Q; ++q) {
+            R a, b;
+            load2(q * nfp + i, q, a, b);
+            sink(q, a, b, i);
+        }
+    } else {
+        uint32_t src[L::Q];
+        const uint32_t mask = pull_sources<L>(g, x, y, z, src);
+#pragma unroll
+        for (int q = 1; q < L::Q; ++q) {
+            const bool fluid = (mask >> q) & 1u;
+            const uint32_t node = fluid ? src[q] : i;
+            const uint32_t off = (fluid ? (uint32_t)q : (uint32_t)L::op(q)) * nfp + node;
+            R a, b;
+            load2(off, q, a, b);
+            sink(q, a, b, fluid ? src[q] : 0xffffffffu);
+        }
+    }
+}
+
 // Both components' incoming populations of node i.  With films (FILM, pull
 // steps only): phase 0 bounces back from films of phase 1 and phase 1 from
 // films of phase 0 (ColorFluid::Run, colorfluid.cpp:155-158), then a film
@@ -129,34 +174,13 @@ __device__ __forceinline__ void color_gather(const Grid& g, const Film& film, co
                                              typename S::R rho_bar = typename S::R(0))
 {
     using R = typename S::R;
-    // One neighbour lookup for both components (the sources are the same).
-    const typename S::T* __restrict__ fin1 = fin + (size_t)L::Q * g.nfp;
-    const uint32_t nfp = g.nfp;
-    const uint32_t nblk = (uint32_t)L::Q * nfp;
-    auto load2 = [&](uint32_t off, int q, R& a, R& b) {
-        if constexpr (IsPacked<S>::value) S::load_pair(fin, off, nblk, q, rho_bar, a, b);
-        else { a = S::load(fin + off, q, R(0)); b = S::load(fin1 + off, q, R(0)); }
-    };
-    load2(i, 0, f0[0], f1[0]);
-    nbr[0] = i;
-    if constexpr (!PULL) {
-#pragma unroll
-        for (int q = 1; q < L::Q; ++q) {
-            load2(q * nfp + i, q, f0[q], f1[q]);
-            nbr[q] = 0;
-        }
-    } else {
-        uint32_t src[L::Q];
-        const uint32_t mask = pull_sources<L>(g, x, y, z, src);
-#pragma unroll
-        for (int q = 1; q < L::Q; ++q) {
-            const bool fluid = (mask >> q) & 1u;
-            const uint32_t node = fluid ? src[q] : i;
-            nbr[L::op(q)] = fluid ? src[q] : 0xffffffffu;
-            const uint32_t off = (fluid ? (uint32_t)q : (uint32_t)L::op(q)) * nfp + node;
-            load2(off, q, f0[q], f1[q]);
-        }
-    }
+    color_pull<L, S, PULL>(g, fin, i, x, y, z, rho_bar, [&](int q, R a, R b, uint32_t src) {
+        f0[q] = a;
+        f1[q] = b;
+        if (q == 0) nbr[0] = i;
+        else if (PULL) nbr[L::op(q)] = src;
+        else nbr[q] = 0;
+    });
     if constexpr (FILM && PULL && !IsPacked<S>::value) {
         const uint32_t b1 = film_sources<L>(g, film.bits[1], x, y, z);   // blocks phase 0
         const uint32_t b0 = film_sources<L>(g, film.bits[0], x, y, z);   // blocks phase 1
@@ -197,7 +221,7 @@ template <class L> constexpr int normal_codes() { return L::D == 3 ? 11 * 11 * 1
 // Pass 1: phase field.  PULL = false reads the node's own values (t = 0).
 template <class L, class S, bool PULL, bool FILM>
 __global__ void __launch_bounds__(128)
-color_phase(const Grid g, const Film film, const typename S::T* __restrict__ fin, double* __restrict__ phi,
+color_phase(const Grid g, const Film film, const typename S::T* __restrict__ fin, double2* __restrict__ dens,
             double* __restrict__ phid, uint32_t* __restrict__ err, const double rho_bar)
 {
     using R = typename S::R;
@@ -219,9 +243,10 @@ color_phase(const Grid g, const Film film, const typename S::T* __restrict__ fin
     // noise of about 1e-5 rho), so its allowance is 1e-3 rho.
     const R tol = sizeof(R) == 8 ? R(1e-10) : (IsPacked<S>::value ? R(1e-3) : R(2.7e-5));
     if (d0 < -tol * dt || d1 < -tol * dt) atomicOr(err, kErrComponent);
-    const double ph = (double)((d0 - d1) / dt);
-    phi[i] = ph;
-    phid[((size_t)z * g.ny + y) * g.nx + x] = ph;
+    // Pass 2 takes the densities from here (exactly the sums it would form
+    // from the same populations) and gathers only the total.
+    dens[i] = make_double2((double)d0, (double)d1);
+    phid[((size_t)z * g.ny + y) * g.nx + x] = (double)((d0 - d1) / dt);
 }
 
 // ColorFluid::colorGradient of node i (colorfluid.cpp:435-570) from the
@@ -327,27 +352,20 @@ __device__ __forceinline__ void color_gradient_node(const ColorWall& W, const ui
 
 }
 
-// Pass 2 for one node whose incoming populations f0, f1 (and the neighbour
-// indices nbr) are gathered: macros, collision, gradient, perturbation and
-// recoloring.  COLL: 0 = SRT, 1 = MRT.
+// Pass 2 for one node from the component densities d0, d1 (sums over
+// q = 0..Q-1 in order) and the total distribution fT = f0 + f1: macros,
+// collision, perturbation and recoloring.  COLL: 0 = SRT, 1 = MRT.
 template <class L, class S, int COLL>
-__device__ __forceinline__ void color_update(const Grid& g, const Force& F, const ColorParams& P,
-                                             typename S::T* __restrict__ fout,
-                                             const typename S::R (&gr)[3], const typename S::R norm,
-                                             const Macros& mo, const int out,
-                                             uint32_t* __restrict__ err, const uint32_t i,
-                                             typename S::R (&f0)[L::Q], typename S::R (&f1)[L::Q])
+__device__ __forceinline__ void color_update_total(const Grid& g, const Force& F, const ColorParams& P,
+                                                   typename S::T* __restrict__ fout,
+                                                   const typename S::R (&gr)[3], const typename S::R norm,
+                                                   const Macros& mo, const int out,
+                                                   uint32_t* __restrict__ err, const uint32_t i,
+                                                   const typename S::R d0, const typename S::R d1,
+                                                   typename S::R (&fT)[L::Q])
 {
     using R = typename S::R;
     // ColorFluid::calcMacroVar (colorfluid.cpp:238-290) and bodyForce (:736-750).
-    // The total distribution fT = f0 + f1 is formed first; afterwards only
-    // fT and the two component densities stay live (register budget).
-    R d0 = f0[0], d1 = f1[0];
-#pragma unroll
-    for (int q = 1; q < L::Q; ++q) { d0 += f0[q]; d1 += f1[q]; }
-    R fT[L::Q];
-#pragma unroll
-    for (int q = 0; q < L::Q; ++q) fT[q] = f0[q] + f1[q];
     const R dt = d0 + d1;
     const R phi_i = (d0 - d1) / dt;
     const R tau = (R(1) + phi_i) * R(P.relax0) + (R(1) - phi_i) * R(P.relax1);
@@ -438,25 +456,78 @@ __device__ __forceinline__ void color_update(const Grid& g, const Force& F, cons
     if (norm > R(1e-9)) {
         const R betaDens01TT = R(P.beta) * dens0T * d1 / dt;
         const R AkNorm = R(P.ak) * norm / tau;
+        // cos(phi_q) = (e_q . gr) / norm, the reference summing the terms
+        // +-gr[d] from 0 in component order and dividing per direction, then
+        // once more by sqrt 2 for a diagonal (colorfluid.cpp:399-428).  IEEE
+        // negation commutes with +, - and /, so a direction's value is the
+        // signed value of one of D axis quotients gr[d]/norm or, for the
+        // diagonal pair (d1 < d2), of (gr[d1] + gr[d2])/norm or
+        // (gr[d1] - gr[d2])/norm: the same values (up to the sign of an exact
+        // zero) from 15 divisions per node instead of 31 in 3D (6 instead of
+        // 13 in 2D).
+        R qa[3], qs[3], qd[3], qs2[3], qd2[3];
+#pragma unroll
+        for (int d = 0; d < L::D; ++d) qa[d] = gr[d] / norm;
+#pragma unroll
+        for (int d1 = 0; d1 < L::D; ++d1)
+#pragma unroll
+            for (int d2 = d1 + 1; d2 < L::D; ++d2) {
+                const int pr = d1 + d2 - 1;
+                qs[pr] = (gr[d1] + gr[d2]) / norm;
+                qd[pr] = (gr[d1] - gr[d2]) / norm;
+                qs2[pr] = qs[pr] / R(1.4142135623730951);
+                qd2[pr] = qd[pr] / R(1.4142135623730951);
+            }
 #pragma unroll
         for (int q = 0; q < L::Q; ++q) {
-            R angle = R(0);
+            int d1 = -1, d2 = -1, s1 = 0, s2 = 0;
 #pragma unroll
             for (int d = 0; d < L::D; ++d) {
                 const int e = comp<L>(q, L::D - 1 - d);
-                if (e == 1) angle += gr[d];
-                else if (e == -1) angle -= gr[d];
+                if (e != 0) {
+                    if (d1 < 0) { d1 = d; s1 = e; }
+                    else { d2 = d; s2 = e; }
+                }
             }
-            angle /= norm;
+            R angle = R(0), cosq = R(0);   // cos(phi_q), and over sqrt 2 for a diagonal
+            if (d1 >= 0 && d2 < 0) {
+                angle = s1 > 0 ? qa[d1] : -qa[d1];
+                cosq = angle;
+            } else if (d2 >= 0) {
+                const int pr = d1 + d2 - 1;
+                // s1 a + s2 b: a + b, a - b, -(a - b), -(a + b).
+                angle = s1 > 0 ? (s2 > 0 ? qs[pr] : qd[pr]) : (s2 > 0 ? -qd[pr] : -qs[pr]);
+                cosq = s1 > 0 ? (s2 > 0 ? qs2[pr] : qd2[pr]) : (s2 > 0 ? -qd2[pr] : -qs2[pr]);
+            }
             fT[q] += AkNorm * (R(w<L>(q)) * angle * angle - R(L::B(q)));
-            if (q != 0 && !axis_dir<L>(q)) angle /= R(1.4142135623730951);
-            const R a0 = dens0T * fT[q] + betaDens01TT * angle * fu0[q];
+            const R a0 = dens0T * fT[q] + betaDens01TT * cosq * fu0[q];
             put(q, a0, fT[q]);
         }
     } else {
 #pragma unroll
         for (int q = 0; q < L::Q; ++q) put(q, dens0T * fT[q], fT[q]);
     }
+}
+
+// Pass 2 for one node from both components' gathered populations f0, f1
+// (the film and Zou-He paths): macros, collision, perturbation and
+// recoloring.  COLL: 0 = SRT, 1 = MRT.
+template <class L, class S, int COLL>
+__device__ __forceinline__ void color_update(const Grid& g, const Force& F, const ColorParams& P,
+                                             typename S::T* __restrict__ fout,
+                                             const typename S::R (&gr)[3], const typename S::R norm,
+                                             const Macros& mo, const int out,
+                                             uint32_t* __restrict__ err, const uint32_t i,
+                                             typename S::R (&f0)[L::Q], typename S::R (&f1)[L::Q])
+{
+    using R = typename S::R;
+    R d0 = f0[0], d1 = f1[0];
+#pragma unroll
+    for (int q = 1; q < L::Q; ++q) { d0 += f0[q]; d1 += f1[q]; }
+    R fT[L::Q];
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) fT[q] = f0[q] + f1[q];
+    color_update_total<L, S, COLL>(g, F, P, fout, gr, norm, mo, out, err, i, d0, d1, fT);
 }
 
 // Colour gradient of node i at (x, y, z) from the dense per-voxel phase
@@ -482,13 +553,22 @@ __device__ __forceinline__ void color_gradient_dense(const Grid& g, const ColorW
 // Pass 2: colour gradient, collision, perturbation and recoloring of every
 // fluid node.  PULL = false is the t = 0 collision.  The gradient comes
 // first, from the dense phase field (its loads hit L2), while the node's
-// population loads are independent of it.  At most 128 registers per thread
-// (four 128-thread blocks per SM): the kernel is latency-bound.
+// population loads are independent of it.  Without films the component
+// densities come from pass 1 and each pulled pair is summed into the total
+// as it arrives, so 19 populations stay live instead of 38.  The kernel is
+// latency-bound; resident 128-thread blocks per SM (CollideBlocks): four for
+// FP64 (128 registers; at five it spills 80 bytes and runs 3 % slower, at
+// six 9 %), six for FP32 arithmetic (80 registers, no spill; 128x128x256
+// medium, FP32 storage 6,880 -> 7,250 fluid MLUPS, 16-bit 5,215 -> 5,470).
+template <class S> struct CollideBlocks { static constexpr int value = 6; };
+template <> struct CollideBlocks<StoreF64> { static constexpr int value = 4; };
+
 template <class L, class S, int COLL, bool PULL, bool FILM>
-__global__ void __launch_bounds__(128, 4)
+__global__ void __launch_bounds__(128, CollideBlocks<S>::value)
 color_collide(const Grid g, const Film film, const Force F, const ColorParams P, const ColorWall W,
               const typename S::T* __restrict__ fin, typename S::T* __restrict__ fout,
-              const double* __restrict__ phid, Macros mo, const int out, uint32_t* __restrict__ err)
+              const double2* __restrict__ dens, const double* __restrict__ phid, Macros mo, const int out,
+              uint32_t* __restrict__ err)
 {
     using R = typename S::R;
     // Blocks run in descending node order: pass 1 has just read the
@@ -501,10 +581,18 @@ color_collide(const Grid g, const Film film, const Force F, const ColorParams P,
     unpack(__ldg(&g.coord[i]), x, y, z);
     R gr[3], norm;
     color_gradient_dense<L, R>(g, W, phid, i, x, y, z, gr, norm);
-    R f0[L::Q], f1[L::Q];
-    uint32_t nbr[L::Q];
-    color_gather<L, S, PULL, FILM>(g, film, fin, i, x, y, z, f0, f1, nbr, R(P.rho_ref[0]));
-    color_update<L, S, COLL>(g, F, P, fout, gr, norm, mo, out, err, i, f0, f1);
+    if constexpr (FILM) {
+        R f0[L::Q], f1[L::Q];
+        uint32_t nbr[L::Q];
+        color_gather<L, S, PULL, FILM>(g, film, fin, i, x, y, z, f0, f1, nbr, R(P.rho_ref[0]));
+        color_update<L, S, COLL>(g, F, P, fout, gr, norm, mo, out, err, i, f0, f1);
+    } else {
+        const double2 d = dens[i];
+        R fT[L::Q];
+        color_pull<L, S, PULL>(g, fin, i, x, y, z, R(P.rho_ref[0]),
+                               [&](int q, R a, R b, uint32_t) { fT[q] = a + b; });
+        color_update_total<L, S, COLL>(g, F, P, fout, gr, norm, mo, out, err, i, R(d.x), R(d.y), fT);
+    }
 }
 
 // ---- two-phase Zou-He boundaries ------------------------------------------------
@@ -606,8 +694,7 @@ __device__ __forceinline__ void color_zou_he_gather(const Grid& g, const Film& f
 template <class L, class S, bool FILM>
 __global__ void __launch_bounds__(128)
 color_zou_he_phase(const Grid g, const Film film, const ZouHe z, const typename S::T* __restrict__ fin,
-                   double* __restrict__ phi, double* __restrict__ phid, uint32_t* __restrict__ err,
-                   const double rho_bar)
+                   double* __restrict__ phid, uint32_t* __restrict__ err, const double rho_bar)
 {
     using R = typename S::R;
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -624,11 +711,11 @@ color_zou_he_phase(const Grid g, const Film film, const ZouHe z, const typename 
     if (!isfinite(d0) || !isfinite(d1) || !isfinite(dt) || !(dt > R(0))) atomicOr(err, kErrDensity);
     const R tol = sizeof(R) == 8 ? R(1e-10) : (IsPacked<S>::value ? R(1e-3) : R(2.7e-5));
     if (d0 < -tol * dt || d1 < -tol * dt) atomicOr(err, kErrComponent);
-    const double ph = (double)((d0 - d1) / dt);
-    phi[i] = ph;
+    // Only the dense phase field: the boundary node's pass-2 result is
+    // replaced by color_zou_he_collide, which sums its own densities.
     int vx, vy, vz;
     unpack(__ldg(&g.coord[i]), vx, vy, vz);
-    phid[((size_t)vz * g.ny + vy) * g.nx + vx] = ph;
+    phid[((size_t)vz * g.ny + vy) * g.nx + vx] = (double)((d0 - d1) / dt);
 }
 
 // Boundary collision pass (after pass 2); also keeps the report's adjacent

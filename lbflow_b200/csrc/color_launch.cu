@@ -16,22 +16,21 @@ void run_step(bool pull, int out, const ColorLaunch& a)
     const unsigned zb = blocks_for(a.zh.n, threads);
     const double rb = a.P.rho_ref[0];
     if (pull)
-        color_phase<L, S, true, FILM><<<blocks, threads, 0, a.stream>>>(a.g, a.film, fin, a.phi, a.phid, a.err, rb);
+        color_phase<L, S, true, FILM><<<blocks, threads, 0, a.stream>>>(a.g, a.film, fin, a.dens, a.phid, a.err, rb);
     else
-        color_phase<L, S, false, false><<<blocks, threads, 0, a.stream>>>(a.g, a.film, fin, a.phi, a.phid, a.err, rb);
+        color_phase<L, S, false, false><<<blocks, threads, 0, a.stream>>>(a.g, a.film, fin, a.dens, a.phid, a.err, rb);
     // Zou-He boundary nodes (PB/VB): their phase from the rebuilt populations
     // before pass 2 reads it, and their collision after pass 2 (overwriting).
     if (pull && zb)
-        color_zou_he_phase<L, S, FILM><<<zb, threads, 0, a.stream>>>(a.g, a.film, a.zh, fin, a.phi, a.phid, a.err,
-                                                                     rb);
+        color_zou_he_phase<L, S, FILM><<<zb, threads, 0, a.stream>>>(a.g, a.film, a.zh, fin, a.phid, a.err, rb);
     if (!pull && zb && (out & kOutAdjacent))
         color_zou_he_record<L, S><<<zb, threads, 0, a.stream>>>(a.g, a.zh, fin, rb);
     if (pull)
         color_collide<L, S, COLL, true, FILM><<<blocks, threads, 0, a.stream>>>(
-            a.g, a.film, a.F, a.P, a.W, fin, fout, a.phid, a.mo, out, a.err);
+            a.g, a.film, a.F, a.P, a.W, fin, fout, a.dens, a.phid, a.mo, out, a.err);
     else
         color_collide<L, S, COLL, false, false><<<blocks, threads, 0, a.stream>>>(
-            a.g, a.film, a.F, a.P, a.W, fin, fout, a.phid, a.mo, out, a.err);
+            a.g, a.film, a.F, a.P, a.W, fin, fout, a.dens, a.phid, a.mo, out, a.err);
     if (pull && zb)
         color_zou_he_collide<L, S, COLL, FILM><<<zb, threads, 0, a.stream>>>(a.g, a.film, a.F, a.P, a.W, a.zh, fin,
                                                                             fout, a.phid, a.mo, out, a.err);

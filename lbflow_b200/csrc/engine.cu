@@ -36,7 +36,8 @@ struct lbf_engine {
     uint8_t* node_phase = nullptr;
     double* label_force = nullptr;
     double *rho0 = nullptr, *rho1 = nullptr, *u = nullptr, *uprev = nullptr, *uadj = nullptr;
-    double *ind = nullptr, *indprev = nullptr, *indadj = nullptr, *phi = nullptr;
+    double *ind = nullptr, *indprev = nullptr, *indadj = nullptr;
+    double2* dens = nullptr;   // two-phase: component densities of the step (pass 1 -> pass 2)
     double* phid = nullptr;         // color: phase field per voxel [N], solid voxels kSolidPhi
     uint16_t* angle_id = nullptr;
     double* angles = nullptr;
@@ -260,7 +261,7 @@ void launch_step(lbf_engine* e, bool pull, int out)
         const bool dither = e->cfg.storage == LBF_STORE_FP16 || e->cfg.storage == LBF_STORE_BF16;
         e->cp.seed = dither && pull ? (++e->steps * 2654435761u) | 1u : 0u;
         ColorWall W{e->angle_id, e->angles, e->tib};
-        ColorLaunch a{grid_of(e), e->force, e->cp, W, fin, fout, e->phi, e->phid, macros_of(e), e->err,
+        ColorLaunch a{grid_of(e), e->force, e->cp, W, fin, fout, e->dens, e->phid, macros_of(e), e->err,
                       e->stream, e->zh, Film{{e->film_bits[0], e->film_bits[1]}}};
         launch_color(e->D, (int)e->cfg.storage, (int)e->cfg.collision, pull, out, a);
     }
@@ -1073,7 +1074,7 @@ int lbf_create(const lbf_config* cfg, const lbf_label labels[256], const uint8_t
         LBF_ALLOC(e->ind, e->nfp);
         LBF_ALLOC(e->indprev, e->nfp);
         LBF_ALLOC(e->indadj, e->nfp);
-        LBF_ALLOC(e->phi, e->nfp);
+        LBF_ALLOC(e->dens, e->nfp);
         LBF_ALLOC(e->phid, e->N);
         fill_value<<<dense_blocks(e->N), 256, 0, e->stream>>>(e->phid, e->N, kSolidPhi);
         LBF_CUDA(cudaGetLastError());
@@ -1103,7 +1104,7 @@ void lbf_destroy(lbf_engine* e)
     if (e->stream) cudaStreamSynchronize(e->stream);
     void* ptrs[] = {e->f[0], e->f[1], e->ex[0], e->ex[1], e->occ, e->coord, e->node_label, e->node_phase, e->label_force,
                     e->rho0, e->rho1, e->u, e->uprev, e->uadj, e->ind, e->indprev, e->indadj,
-                    e->phi, e->angle_id, e->angles, e->tib, e->err, e->partial, e->red,
+                    e->dens, e->angle_id, e->angles, e->tib, e->err, e->partial, e->red,
                     e->zh_node, e->zh_code, e->zh_value, e->zh_num, e->dense_tmp, e->film_bits[0], e->film_bits[1],
                     e->stage, e->phid, e->solid_f[0], e->solid_f[1]};
     for (void* p : ptrs) if (p) cudaFreeAsync(p, e->stream);

@@ -29,8 +29,8 @@ struct ColorLaunch {
     ColorWall W;
     const void* fin;   // [2][Q][nfp]
     void* fout;
-    double* phi;       // [nfp] phase field of this step (written by pass 1)
-    double* phid;      // [N] the same phase field per voxel (solid voxels: kSolidPhi)
+    double2* dens;     // [nfp] component densities (rho0, rho1) of this step (written by pass 1)
+    double* phid;      // [N] phase field (rho0 - rho1)/rho per voxel (solid voxels: kSolidPhi)
     Macros mo;
     uint32_t* err;
     cudaStream_t stream;
