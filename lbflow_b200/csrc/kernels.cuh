@@ -99,35 +99,55 @@ __device__ __forceinline__ float dither_bits(float x, uint32_t r, int drop)
     return __uint_as_float(__float_as_uint(x) + (r >> (32 - drop)));
 }
 
-template <class L> struct StoreF16 {
+// Stochastic rounding of two floats to a 16-bit pair in one instruction
+// (cvt.rs, sm_100a): the low half (lo) takes the random bits 0..12 of rbits
+// for IEEE half, 0..15 for bfloat16; the high half (hi) bits 16..28 / 16..31.
+// A value rounds away from zero with probability equal to the discarded
+// fraction (subnormals included); satfinite saturates at the largest finite
+// value, as truncation does.
+__device__ __forceinline__ uint32_t pack_sr(__half, float hi, float lo, uint32_t rbits)
+{
+    uint32_t d;
+    asm("cvt.rs.satfinite.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rbits));
+    return d;
+}
+__device__ __forceinline__ uint32_t pack_sr(__nv_bfloat16, float hi, float lo, uint32_t rbits)
+{
+    uint32_t d;
+    asm("cvt.rs.satfinite.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rbits));
+    return d;
+}
+
+// Shifted 16-bit float storage (H: __half or __nv_bfloat16).
+template <class L, class H> struct StoreShifted16 {
     static constexpr bool blocked = false;
     static constexpr bool dither = true;
-    using T = __half;
+    using T = H;
     using R = float;
     static constexpr bool shifted = true;
-    __device__ static R load(const T* p, int q, R) { return __half2float(__ldg(p)) * ShiftScale<L>::inv(q); }
-    __device__ static void store(T* p, R v, int q, R) { *p = __float2half_rn(v * ShiftScale<L>::scale(q)); }
-    // Normal half range only (|x| >= 2^-14, 13 discarded bits); below it the
-    // subnormal spacing is fixed and round-to-nearest is kept.
-    __device__ static void store_sr(T* p, R v, int q, uint32_t r)
+    // The scaling product is rounded on its own (never fused into the sums
+    // that consume it), so every kernel inlining this load -- the single
+    // and the batched step -- computes bitwise the same fields.
+    __device__ static R load(const T* p, int q, R)
     {
-        const float x = v * ShiftScale<L>::scale(q);
-        *p = fabsf(x) >= 6.103515625e-05f ? __float2half_rz(dither_bits(x, r, 13)) : __float2half_rn(x);
+        return __fmul_rn(float(__ldg(p)), ShiftScale<L>::inv(q));
+    }
+    __device__ static void store(T* p, R v, int q, R) { *p = T(v * ShiftScale<L>::scale(q)); }
+    // Directions qa (low half) and qb (high half) rounded together; rbits
+    // carries 16 random bits for each.
+    __device__ static void store_sr2(T* pa, T* pb, R va, R vb, int qa, int qb, uint32_t rbits)
+    {
+        const uint32_t d = pack_sr(H(0.0f), vb * ShiftScale<L>::scale(qb), va * ShiftScale<L>::scale(qa), rbits);
+        *reinterpret_cast<uint16_t*>(pa) = (uint16_t)d;
+        *reinterpret_cast<uint16_t*>(pb) = (uint16_t)(d >> 16);
+    }
+    __device__ static void store_sr1(T* p, R v, int q, uint32_t rbits)
+    {
+        *reinterpret_cast<uint16_t*>(p) = (uint16_t)pack_sr(H(0.0f), 0.0f, v * ShiftScale<L>::scale(q), rbits);
     }
 };
-template <class L> struct StoreBF16 {
-    static constexpr bool blocked = false;
-    static constexpr bool dither = true;
-    using T = __nv_bfloat16;
-    using R = float;
-    static constexpr bool shifted = true;
-    __device__ static R load(const T* p, int q, R) { return __bfloat162float(__ldg(p)) * ShiftScale<L>::inv(q); }
-    __device__ static void store(T* p, R v, int q, R) { *p = __float2bfloat16_rn(v * ShiftScale<L>::scale(q)); }
-    __device__ static void store_sr(T* p, R v, int q, uint32_t r)
-    {
-        *p = __float2bfloat16_rz(dither_bits(v * ShiftScale<L>::scale(q), r, 16));
-    }
-};
+template <class L> using StoreF16 = StoreShifted16<L, __half>;
+template <class L> using StoreBF16 = StoreShifted16<L, __nv_bfloat16>;
 template <class L> struct StoreF32 {
     static constexpr bool blocked = false;
     static constexpr bool dither = false;
@@ -309,10 +329,19 @@ struct Trt { double sp, sm; };
 // (single phase: A = 0, B = rho - 1.5 rho0 u^2, C = 4.5 rho0, K = 3 rho0;
 //  color: A = feq_u0, B = -1.5 rho u^2, C = 4.5 rho, K = 3 rho) and the Guo
 // source as w_q (3 (e.F - u.F) + 9 (e.u)(e.F)).
+template <class L, bool HAS_A>
+__device__ __forceinline__ void collide_trt_x2(float (&f)[L::Q], const float* A, float B, float C, float K,
+                                               const float (&u)[3], const float (&F)[3], float uf, float sp,
+                                               float sm);
+
 template <class L, class R, bool HAS_A>
 __device__ __forceinline__ void collide_trt(R (&f)[L::Q], const R* A, R B, R C, R K,
                                             const R (&u)[3], const R (&F)[3], R uf, R sp, R sm)
 {
+    if constexpr (sizeof(R) == 4) {
+        collide_trt_x2<L, HAS_A>(f, A, B, C, K, u, F, uf, sp, sm);
+        return;
+    }
     const R hp = R(1) - R(0.5) * sp, hm = R(1) - R(0.5) * sm;
     {
         const R w0 = R(w<L>(0));
@@ -333,6 +362,73 @@ __device__ __forceinline__ void collide_trt(R (&f)[L::Q], const R* A, R B, R C, 
         const R od = -sm * (fm - feqm) + hm * (wq * R(3) * ef);
         f[q] += ev + od;
         f[o] += ev - od;
+    }
+}
+
+// e_q . v with the direction's components known at compile time.
+template <class L> __device__ __forceinline__ float dot_e(int q, const float (&v)[3])
+{
+    float s = 0.0f;
+    if (L::ex(q)) s = L::ex(q) > 0 ? v[0] : -v[0];
+    if (L::ey(q)) s = L::ey(q) > 0 ? s + v[1] : s - v[1];
+    if (L::ez(q)) s = L::ez(q) > 0 ? s + v[2] : s - v[2];
+    return s;
+}
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
+
+// The two-rate update in FP32 arithmetic, two opposite pairs per instruction
+// with the packed FP32 operations of sm_100 (__ffma2_rn, __fadd2_rn,
+// __fmul2_rn: each lane rounds as the scalar operation does).  The FP32
+// storages are issue-bound, and this halves the collision's share of the
+// issued instructions.
+template <class L, bool HAS_A>
+__device__ __forceinline__ void collide_trt_x2(float (&f)[L::Q], const float* A, float B, float C, float K,
+                                               const float (&u)[3], const float (&F)[3], float uf, float sp,
+                                               float sm)
+{
+    const float hp = 1.0f - 0.5f * sp, hm = 1.0f - 0.5f * sm;
+    {
+        const float w0 = float(w<L>(0));
+        const float feq0 = (HAS_A ? A[0] : 0.0f) + w0 * B;
+        f[0] += -sp * (f[0] - feq0) + hp * (w0 * (-3.0f * uf));
+    }
+    const float2 B2 = dup2(B), C2 = dup2(C), K2 = dup2(K), nsp = dup2(-sp), nsm = dup2(-sm);
+    const float2 hp2 = dup2(hp), hm2 = dup2(hm), m3uf = dup2(-3.0f * uf), half = dup2(0.5f), nine = dup2(9.0f);
+#pragma unroll
+    for (int p = 0; p < L::NPAIR; p += 2) {
+        if (p + 1 < L::NPAIR) {
+            const int qa = L::pair(p), oa = L::op(qa), qb = L::pair(p + 1), ob = L::op(qb);
+            const float2 eu = make_float2(dot_e<L>(qa, u), dot_e<L>(qb, u));
+            const float2 ef = make_float2(dot_e<L>(qa, F), dot_e<L>(qb, F));
+            const float2 wq = make_float2(float(w<L>(qa)), float(w<L>(qb)));
+            const float2 w3 = make_float2(float(3.0 * w<L>(qa)), float(3.0 * w<L>(qb)));
+            float2 feqp = __fmul2_rn(wq, __ffma2_rn(C2, __fmul2_rn(eu, eu), B2));
+            if (HAS_A) feqp = __fadd2_rn(make_float2(A[qa], A[qb]), feqp);
+            const float2 feqm = __fmul2_rn(__fmul2_rn(wq, K2), eu);
+            const float2 fq = make_float2(f[qa], f[qb]), fo = make_float2(f[oa], f[ob]);
+            const float2 fp = __fmul2_rn(half, __fadd2_rn(fq, fo));
+            const float2 fm = __fmul2_rn(half, __fadd2_rn(fq, neg2(fo)));
+            const float2 srcp = __fmul2_rn(__fmul2_rn(hp2, wq), __ffma2_rn(nine, __fmul2_rn(eu, ef), m3uf));
+            const float2 srcm = __fmul2_rn(__fmul2_rn(hm2, w3), ef);
+            const float2 ev = __ffma2_rn(nsp, __fadd2_rn(fp, neg2(feqp)), srcp);
+            const float2 od = __ffma2_rn(nsm, __fadd2_rn(fm, neg2(feqm)), srcm);
+            const float2 nq = __fadd2_rn(fq, __fadd2_rn(ev, od));
+            const float2 no = __fadd2_rn(fo, __fadd2_rn(ev, neg2(od)));
+            f[qa] = nq.x; f[qb] = nq.y;
+            f[oa] = no.x; f[ob] = no.y;
+        } else {
+            const int q = L::pair(p), o = L::op(q);
+            const float eu = dot_e<L>(q, u), ef = dot_e<L>(q, F), wq = float(w<L>(q));
+            const float feqp = (HAS_A ? A[q] : 0.0f) + wq * (B + C * eu * eu);
+            const float feqm = wq * K * eu;
+            const float fp = 0.5f * (f[q] + f[o]);
+            const float fm = 0.5f * (f[q] - f[o]);
+            const float ev = -sp * (fp - feqp) + hp * (wq * (9.0f * eu * ef - 3.0f * uf));
+            const float od = -sm * (fm - feqm) + hm * (wq * 3.0f * ef);
+            f[q] += ev + od;
+            f[o] += ev - od;
+        }
     }
 }
 
@@ -426,13 +522,22 @@ __device__ __forceinline__ void scsp_update(const Grid& g, const Force& F, const
         S::store_blk(fout, g.nfp, i, f, eout);
     } else if constexpr (S::dither) {
         if (P.seed) {
-            // One linear congruential stream per node and step; its high bits
-            // are the rounding offsets.
+            // One linear congruential stream per node and step, one draw per
+            // direction; the high 16 bits of each draw are its rounding
+            // offsets (a pair of directions takes the high halves of two
+            // draws, the first in bits 0..15).
             uint32_t r = hash32((i - P.node0) * 0x9e3779b9u + P.seed);
 #pragma unroll
-            for (int q = 0; q < L::Q; ++q) {
+            for (int q = 0; q < L::Q; q += 2) {
                 r = r * 1664525u + 1013904223u;
-                S::store_sr(fout + (q * g.nfp + i), f[q], q, r);
+                const uint32_t ra = r;
+                if (q + 1 < L::Q) {
+                    r = r * 1664525u + 1013904223u;
+                    S::store_sr2(fout + (q * g.nfp + i), fout + ((q + 1) * g.nfp + i), f[q], f[q + 1], q, q + 1,
+                                 __byte_perm(ra, r, 0x7632));
+                } else {
+                    S::store_sr1(fout + (q * g.nfp + i), f[q], q, ra >> 16);
+                }
             }
         } else {
 #pragma unroll
