@@ -80,7 +80,7 @@ batch_step(const BatchGeom* __restrict__ geoms, const Tile* __restrict__ tiles, 
         P.seed = seed;
         P.node0 = G.node_base;
         for (uint32_t k = threadIdx.x; k < tl.count; k += blockDim.x)
-            scsp_update<L, S, PULL>(g, F, P, fin, fout, tl.first + k, mo, out, err, nullptr, nullptr);
+            scsp_update<L, S, PULL, true>(g, F, P, fin, fout, tl.first + k, mo, out, err, nullptr, nullptr);
     }
 }
 

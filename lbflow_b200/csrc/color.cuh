@@ -149,7 +149,7 @@ __device__ __forceinline__ void color_pull(const Grid& g, const typename S::T* _
         }
     } else {
         uint32_t src[L::Q];
-        const uint32_t mask = pull_sources<L>(g, x, y, z, src);
+        const uint32_t mask = pull_sources<L, (sizeof(R) == 4)>(g, x, y, z, src);
 #pragma unroll
         for (int q = 1; q < L::Q; ++q) {
             const bool fluid = (mask >> q) & 1u;

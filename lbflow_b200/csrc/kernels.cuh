@@ -231,14 +231,30 @@ __device__ __forceinline__ typename S::R load_pop(const typename S::T* p, int q,
 // Pull sources of every direction: src[q] = compact index of voxel x - e_q
 // and bit q of the returned mask set when that voxel is fluid.  The sources
 // lie in (at most) nine x-rows (y - ey, z - ez); each row's occupancy word
-// around x is loaded once and x - 1, x, x + 1 are read from it, falling back
-// to a separate lookup only at a word boundary or the periodic wrap in x.
-template <class L>
+// at x is loaded once for the sources at x.  The sources at x - 1 and x + 1
+// (periodic in x) come in two forms:
+//   UNIFORM = true:  looked up in the word that holds them (the same word
+//                    except at a word boundary or the wrap) by one
+//                    branch-free formula, so a warp's lanes never split;
+//   UNIFORM = false: read from the row word at x, with a separate lookup only
+//                    at a word boundary or the wrap (fewer loads and
+//                    registers, but most warps take both sides of the split).
+// The indices are the same either way.  Which is faster depends on the
+// kernel: the FP64 single-geometry step (latency-bound at 72 registers) runs
+// 9 % slower uniform; the FP32-arithmetic steps (issue-bound) run 4-12 %
+// faster uniform (FP16 storage 28,230 -> 31,230 fluid MLUPS on the 256^3
+// cube) and the batched FP64 step 5 % faster.
+template <class L, bool UNIFORM>
 __device__ __forceinline__ uint32_t pull_sources(const Grid& g, int x, int y, int z, uint32_t (&src)[L::Q])
 {
     const int b = x & 31;
     const int wx = x >> 5;
     const uint32_t below = (1u << b) - 1u;
+    const int xl = x == 0 ? g.nx - 1 : x - 1;
+    const int xr = x + 1 == g.nx ? 0 : x + 1;
+    const int wl = xl >> 5, wr = xr >> 5;
+    const uint32_t bl = xl & 31, br = xr & 31;
+    const uint32_t belowl = (1u << bl) - 1u, belowr = (1u << br) - 1u;
     uint32_t mask = 0;
     uint32_t rbase[9], ridx[9], rbits[9];
     bool rload[9] = {false, false, false, false, false, false, false, false, false};
@@ -264,6 +280,10 @@ __device__ __forceinline__ uint32_t pull_sources(const Grid& g, int x, int y, in
         if (dx == 0) {
             fl = (bits >> b) & 1u;
             idx = ridx[r];
+        } else if (UNIFORM) {
+            const uint2 e = __ldg(&g.occ[rbase[r] + (dx < 0 ? wl : wr)]);
+            fl = (e.x >> (dx < 0 ? bl : br)) & 1u;
+            idx = e.y + __popc(e.x & (dx < 0 ? belowl : belowr));
         } else if (dx < 0 && b > 0) {
             fl = (bits >> (b - 1)) & 1u;
             idx = ridx[r] - fl;
@@ -271,9 +291,8 @@ __device__ __forceinline__ uint32_t pull_sources(const Grid& g, int x, int y, in
             fl = (bits >> (b + 1)) & 1u;
             idx = ridx[r] + ((bits >> b) & 1u);
         } else {
-            const int sx = wrap(x + dx, g.nx);
-            const uint2 e = __ldg(&g.occ[rbase[r] + (sx >> 5)]);
-            const uint32_t sb = sx & 31;
+            const uint2 e = __ldg(&g.occ[rbase[r] + (dx < 0 ? wl : wr)]);
+            const uint32_t sb = dx < 0 ? bl : br;
             fl = (e.x >> sb) & 1u;
             idx = e.y + __popc(e.x & ((1u << sb) - 1u));
         }
@@ -283,7 +302,7 @@ __device__ __forceinline__ uint32_t pull_sources(const Grid& g, int x, int y, in
     return mask;
 }
 
-template <class L, class S, bool PULL>
+template <class L, class S, bool PULL, bool UNIFORM = (sizeof(typename S::R) == 4)>
 __device__ __forceinline__ void gather(const Grid& g, const typename S::T* __restrict__ fin,
                                        uint32_t i, int x, int y, int z,
                                        typename S::R (&f)[L::Q], uint32_t (&nbr)[L::Q],
@@ -300,7 +319,7 @@ __device__ __forceinline__ void gather(const Grid& g, const typename S::T* __res
         return;
     }
     uint32_t src[L::Q];
-    const uint32_t mask = pull_sources<L>(g, x, y, z, src);
+    const uint32_t mask = pull_sources<L, UNIFORM>(g, x, y, z, src);
 #pragma unroll
     for (int q = 1; q < L::Q; ++q) {
         const bool fluid = (mask >> q) & 1u;
@@ -458,7 +477,7 @@ __device__ __forceinline__ uint32_t hash32(uint32_t x)
 
 // Update of one fluid node i (the body of scsp_step, shared with the batched
 // kernel).
-template <class L, class S, bool PULL>
+template <class L, class S, bool PULL, bool UNIFORM = (sizeof(typename S::R) == 4)>
 __device__ __forceinline__ void scsp_update(const Grid& g, const Force& F, const ScspParams& P,
                                             const typename S::T* __restrict__ fin,
                                             typename S::T* __restrict__ fout, const uint32_t i,
@@ -471,7 +490,7 @@ __device__ __forceinline__ void scsp_update(const Grid& g, const Force& F, const
     const R rho0 = R(P.rho0);
     R f[L::Q];
     uint32_t nbr[L::Q];
-    gather<L, S, PULL>(g, fin, i, x, y, z, f, nbr, rho0, ein);
+    gather<L, S, PULL, UNIFORM>(g, fin, i, x, y, z, f, nbr, rho0, ein);
 
     R Fv[3];
     if (F.uniform) { Fv[0] = R(F.fx); Fv[1] = R(F.fy); Fv[2] = R(F.fz); }
